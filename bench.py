@@ -1,0 +1,411 @@
+"""Benchmark: FD stencil throughput on the kernel-microbench workload.
+
+Workload ("step"): one application of the order-6 (nn=3, 19-point) kinetic
+Laplacian  -1/2 nabla^2  to a batch of 256 grids of 96x96x96 float64 points
+(h = 0.2 A, periodic), values from a seeded N(0, 1) -- the
+(256, 96, 96, 96) kernel-microbench configuration.  Metric: algorithmic
+bytes moved per second, 2 * 256 * 96^3 * 8 B per step (one read + one write
+of the array; halos and coefficients excluded).  Inputs (3.6 GB) are larger
+than the 126 MB L2, so no flush is needed between steps.
+
+Also reported on the same JSON line:
+  suite        the other microbench kernels (FP32, zero boundaries, Gradient,
+               restriction / interpolation k=2, 6, the V-cycle), GB/s each
+  roofline     the stencil kernel against the measured HBM copy bandwidth
+  e2e          the same metric through the public API with host buffers
+               (pinned H2D copy + apply + D2H copy inside the timed region)
+  cpu_baseline GPAW's own C Operator (built from the reference sources into
+               oracle/_ref) on the host cores, bounded sample of 16 grids
+
+`--impl reference` times GPAW's own C implementation of the same step on the
+host cores (all threads) and prints the same metric with "impl": "reference".
+Multi-GPU (`--gpus N` under torchrun): independent replicas (the path has no
+exchange step on one grid per band batch), value = total bytes / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+BOHR = 0.52917721
+NB, N = 256, 96
+H_ANG = 0.2
+METRIC = 'FD stencil GB/s: order-6 Laplacian on (256,96,96,96)'
+
+
+def peaks():
+    p = REPO / 'MEASURED_PEAKS.json'
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+def profiled_traffic():
+    """dram bytes per launch of the stencil kernel from the committed ncu
+    summary (profiles/star_kernel_f64_laplace_256x96.txt), or None."""
+    p = REPO / 'profiles' / 'star_kernel_f64_laplace_256x96.txt'
+    if not p.exists():
+        return None
+    m = re.search(r'traffic_bytes_per_launch\s*=\s*([0-9.eE+]+)', p.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,'
+              'clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,'
+              'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device_index):
+        self.lines = []
+        self.proc = None
+        self.dev = device_index
+
+    def start(self):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            ident = uuid if uuid.startswith('GPU-') else 'GPU-' + uuid
+        except Exception:
+            ident = str(self.dev)
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', ident, f'--query-gpu={self.FIELDS}',
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+                 'sw_power_cap']
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[4:8]):
+                if v.lower() == 'active':
+                    reasons.add(name)
+        return {'sm_mhz': float(np.median(sm)) if sm else None,
+                'sm_max_mhz': smax, 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def grid(pbc, n=N):
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    N_c = np.array([n, n, n]) + (0 if pbc else 1)
+    return GridDescriptor(N_c, N_c * H_ANG / BOHR, pbc)
+
+
+def time_launches(fn, reps, stream):
+    """Average device time of `fn` (one launch chain) with CUDA events on the
+    launching stream."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(reps)]
+    for a, b in ev:
+        a.record(stream)
+        fn()
+        b.record(stream)
+    torch.cuda.synchronize()
+    return float(np.mean([a.elapsed_time(b) for a, b in ev]))
+
+
+def suite(torch, stream):
+    """GB/s of the other kernel-microbench kernels (algorithmic bytes)."""
+    from gpaw_b200.fd_operators import Laplace, Gradient
+    from gpaw_b200.transformers import Transformer
+    from gpaw_b200.preconditioner import Preconditioner
+    out = {}
+    g = torch.Generator(device='cuda').manual_seed(1)
+    for dtype, dname in ((torch.float64, 'f64'), (torch.float32, 'f32')):
+        for pbc in (True, False):
+            gd = grid(pbc)
+            x = torch.randn((NB,) + tuple(gd.n_c), generator=g, device='cuda', dtype=dtype)
+            y = torch.empty_like(x)
+            nbytes = 2 * x.numel() * x.element_size()
+            bc = 'periodic' if pbc else 'zero'
+            lap = Laplace(gd, -0.5, 3)
+            lap.apply(x, y)
+            t = time_launches(lambda: lap.apply(x, y), 5, stream)
+            out[f'laplace_nn3_{dname}_{bc}'] = round(nbytes / t / 1e6, 1)
+            grad = Gradient(gd, 0, 1.0, 3)
+            grad.apply(x, y)
+            t = time_launches(lambda: grad.apply(x, y), 5, stream)
+            out[f'gradient_nn3_{dname}_{bc}'] = round(nbytes / t / 1e6, 1)
+            if dtype == torch.float64:
+                # restrict / interpolate: zero boundaries use n = 95 -> 47
+                gdf = grid(pbc) if pbc else grid(False, N - 1)
+                gdc = gdf.coarsen()
+                xf = x if pbc else torch.randn((NB,) + tuple(gdf.n_c), generator=g,
+                                               device='cuda', dtype=dtype)
+                xc = torch.empty((NB,) + tuple(gdc.n_c), device='cuda', dtype=dtype)
+                yf = torch.empty_like(xf)
+                rbytes = (xf.numel() + xc.numel()) * 8
+                for nn in (1, 3):
+                    r = Transformer(gdf, gdc, nn)
+                    r.apply(xf, xc)
+                    t = time_launches(lambda: r.apply(xf, xc), 5, stream)
+                    out[f'restrict_k{2 * nn}_{dname}_{bc}'] = round(rbytes / t / 1e6, 1)
+                    it = Transformer(gdc, gdf, nn)
+                    it.apply(xc, yf)
+                    t = time_launches(lambda: it.apply(xc, yf), 5, stream)
+                    out[f'interpolate_k{2 * nn}_{dname}_{bc}'] = round(rbytes / t / 1e6, 1)
+                del xf, xc, yf
+            del x, y
+    # V-cycle on 160 bands of the Si64 grid (56^3, periodic), FP64
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    gd = GridDescriptor((56, 56, 56), (20.52, 20.52, 20.52), True)
+    kin = Laplace(gd, -0.5, 3)
+    P = Preconditioner(gd, kin, float, block=10)
+    R = torch.randn((160, 56, 56, 56), generator=g, device='cuda', dtype=torch.float64)
+    d = torch.empty_like(R)
+    P(R, out=d)
+    t = time_launches(lambda: P(R, out=d), 5, stream)
+    out['precond_vcycle_f64_56cubed_160bands_ms'] = round(t, 3)
+    out['precond_vcycle_f64_min_bytes_GBps'] = round(2 * R.numel() * 8 / t / 1e6, 1)
+    return out
+
+
+def cpu_reference_rate(nb_sample, threads, reps=3):
+    """GPAW's own C Operator (oracle/_ref) on the host: best-of GB/s."""
+    from oracle import ref, fd
+    if not ref.available():
+        return None
+    gd = grid(True)
+    coefs, offs = fd.guc_laplace(gd.h_cv, -0.5, 3)
+    op = ref.operator(coefs, offs, gd.n_c, (1, 1, 1), True)
+    rng = np.random.default_rng(0)
+    a = rng.standard_normal((nb_sample,) + tuple(gd.n_c))
+    b = np.zeros_like(a)
+    op.apply(a, b)
+    best = 1e30
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        op.apply(a, b)
+        best = min(best, time.perf_counter() - t0)
+    return 2 * a.nbytes / best / 1e9, best
+
+
+def run_reference(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({'impl': 'reference', 'unavailable':
+                          'oracle/_ref (GPAW C extension from the reference '
+                          'sources) was not built'}))
+        return
+    nb = 16
+    from oracle import fd
+    gd = grid(True)
+    coefs, offs = fd.guc_laplace(gd.h_cv, -0.5, 3)
+    op = ref.operator(coefs, offs, gd.n_c, (1, 1, 1), True)
+    rng = np.random.default_rng(0)
+    a = rng.standard_normal((nb,) + tuple(gd.n_c))
+    b = np.zeros_like(a)
+    for _ in range(args.warmup):
+        op.apply(a, b)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        op.apply(a, b)
+    t = time.perf_counter() - t0
+    value = 2 * a.nbytes * args.steps / t / 1e9
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': round(value, 2),
+        'unit': 'GB/s', 'n_gpus': args.gpus, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': round(t / args.steps * 1e3, 3),
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f64', 'data': 'synthetic N(0,1), seed 0',
+        'config': {'workload': 'laplace_nn3_f64_periodic_256x96^3',
+                   'sample': f'{nb} of 256 grids per step'},
+        'cpu_baseline': {'value': round(value, 2), 'unit': 'GB/s',
+                         'cores': threads, 'kind': 'reference',
+                         'sample': f'{nb} grids of 96^3 per step'},
+        'e2e': {'value': round(value, 2), 'unit': 'GB/s',
+                'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--no-suite', action='store_true')
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count() or 1))
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group('nccl', timeout=timedelta(seconds=120),
+                                device_id=torch.device('cuda', local))
+    from gpaw_b200.fd_operators import Laplace
+    stream = torch.cuda.current_stream()
+    gd = grid(True)
+    lap = Laplace(gd, -0.5, 3)
+    g = torch.Generator(device='cuda').manual_seed(0)
+    x = torch.randn((NB, N, N, N), generator=g, device='cuda', dtype=torch.float64)
+    y = torch.empty_like(x)
+    nbytes = 2 * x.numel() * 8
+
+    for _ in range(max(args.warmup, 3)):
+        lap.apply(x, y)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for a, b in ev:
+        a.record(stream)
+        lap.apply(x, y)
+        b.record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    launch_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    if world > 1:
+        t = torch.tensor([total_ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = t.item()
+    value = world * nbytes * args.steps / (total_ms / 1e3) / 1e9
+
+    # e2e through the public API with host buffers (pinned), fewer steps
+    e2e_steps = min(args.steps, 3)
+    xh = x.cpu().pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    xd = torch.empty_like(x)
+    yd = torch.empty_like(x)
+    xd.copy_(xh, non_blocking=True)
+    lap.apply(xd, yd)
+    yh.copy_(yd, non_blocking=True)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        xd.copy_(xh, non_blocking=True)
+        lap.apply(xd, yd)
+        yh.copy_(yd, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    del xd, yd
+    if world > 1:
+        t = torch.tensor([e2e_ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = t.item()
+    e2e_value = world * nbytes / (e2e_ms / 1e3) / 1e9
+
+    suite_res = None
+    if not args.no_suite:
+        del x, y
+        torch.cuda.empty_cache()
+        suite_res = suite(torch, stream)
+
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        r = cpu_reference_rate(16, threads)
+        if r is not None:
+            cpu = {'value': round(r[0], 2), 'unit': 'GB/s', 'cores': threads,
+                   'kind': 'reference',
+                   'sample': '16 grids of 96^3 FP64 periodic, best of 3 '
+                             '(GPAW C Operator from the reference sources, '
+                             f'OpenMP {os.environ.get("OMP_NUM_THREADS", "default")} threads)'}
+
+    peak, peak_kind = peaks()
+    achieved = nbytes / (launch_ms / 1e3) / 1e9
+    traffic = profiled_traffic()
+    line = {
+        'metric': METRIC, 'value': round(value, 1), 'unit': 'GB/s',
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': round(total_ms / args.steps, 4),
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f64', 'data': 'synthetic N(0,1), seeded (torch.Generator seed 0)',
+        'config': {'workload': 'laplace_nn3_f64_periodic_256x96^3',
+                   'grid': [NB, N, N, N], 'h_angstrom': H_ANG,
+                   'stencil': '19-point order-6 kinetic Laplacian',
+                   'l2': 'inputs 1.8 GB > L2, no flush',
+                   'parallelism': f'replicas x{world}'},
+        'clocks': clk,
+        'e2e': {'value': round(e2e_value, 2), 'unit': 'GB/s',
+                'h2d_bytes_per_step': NB * N**3 * 8,
+                'd2h_bytes_per_step': NB * N**3 * 8,
+                'steps': e2e_steps},
+        'gpu_launches': args.steps,
+        'roofline': {'bound': 'hbm', 'achieved': round(achieved, 1),
+                     'peak': peak, 'unit': 'GB/s', 'frac': round(achieved / peak, 4),
+                     'peak_kind': peak_kind,
+                     'traffic': traffic,
+                     'kernel': 'star_kernel<double,H=3>'},
+        'cpu_baseline': cpu,
+        'suite_GBps': suite_res,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,118 @@
+"""ctypes binding of libgpawb200.so (the C ABI declared in include/gpawb200.h).
+
+The library is built in-tree (gpaw_b200/build.py).  There is no fallback:
+if the library is missing or a call fails, a GPAWB200Error is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import c_double, c_int, c_int64, c_void_p, c_char_p, POINTER
+from pathlib import Path
+
+import numpy as np
+import torch
+
+LIBPATH = Path(__file__).resolve().with_name('libgpawb200.so')
+
+GB_DTYPE = {torch.float64: 0, torch.float32: 1,
+            torch.complex128: 2, torch.complex64: 3}
+
+
+class GPAWB200Error(RuntimeError):
+    pass
+
+
+_lib = None
+
+P64 = POINTER(c_int64)
+PD = POINTER(c_double)
+
+# name -> (restype, argtypes); mirrors include/gpawb200.h
+_SIGNATURES = {
+    'gb_last_error': (c_char_p, []),
+    'gb_version': (c_char_p, []),
+    'gb_device_sm_count': (c_int, [POINTER(c_int)]),
+    'gb_operator_new': (c_int, [PD, P64, c_int, P64, c_int, P64, c_int, c_int,
+                                POINTER(c_void_p)]),
+    'gb_operator_apply': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int,
+                                  PD, c_void_p]),
+    'gb_operator_relax': (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int,
+                                  c_double, c_void_p]),
+    'gb_operator_get_diagonal_element': (c_int, [c_void_p, PD]),
+    'gb_operator_free': (c_int, [c_void_p]),
+    'gb_transformer_new': (c_int, [P64, P64, c_int, P64, P64, P64, P64, c_int,
+                                   c_int, POINTER(c_void_p)]),
+    'gb_transformer_apply': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,
+                                     c_int, PD, c_void_p]),
+    'gb_transformer_free': (c_int, [c_void_p]),
+    'gb_fd_precond': (c_int, [c_void_p] * 7 + [c_void_p] * 8 +
+                      [c_void_p, c_void_p, c_double, c_int64, c_int, PD,
+                       c_void_p]),
+}
+
+
+def lib():
+    """Load (once) and return the ctypes handle of libgpawb200.so."""
+    global _lib
+    if _lib is None:
+        if not LIBPATH.exists():
+            raise GPAWB200Error(
+                f'{LIBPATH} is missing: build it with `python -m gpaw_b200.build`'
+                ' (there is no CPU fallback)')
+        h = ctypes.CDLL(str(LIBPATH))
+        for name, (res, args) in _SIGNATURES.items():
+            f = getattr(h, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = h
+    return _lib
+
+
+def check(status: int, what: str = '') -> None:
+    if status != 0:
+        msg = lib().gb_last_error().decode(errors='replace')
+        raise GPAWB200Error(f'{what}: status {status}: {msg}')
+
+
+def i64(values) -> ctypes.Array:
+    a = np.ascontiguousarray(np.asarray(values, dtype=np.int64).ravel())
+    return (c_int64 * len(a))(*a.tolist())
+
+
+def f64(values) -> ctypes.Array:
+    a = np.ascontiguousarray(np.asarray(values, dtype=np.float64).ravel())
+    return (c_double * len(a))(*a.tolist())
+
+
+def phases(phase_cd) -> ctypes.Array | None:
+    """3x2 complex Bloch phases -> 12 doubles (re, im) or None."""
+    if phase_cd is None:
+        return None
+    if isinstance(phase_cd, torch.Tensor):
+        phase_cd = phase_cd.detach().cpu().numpy()
+    p = np.asarray(phase_cd, dtype=complex).reshape(3, 2)
+    return f64(np.stack([p.real, p.imag], axis=-1))
+
+
+def dtype_code(t: torch.Tensor) -> int:
+    try:
+        return GB_DTYPE[t.dtype]
+    except KeyError:
+        raise GPAWB200Error(f'unsupported dtype {t.dtype}') from None
+
+
+def stream_of(t: torch.Tensor) -> int:
+    return torch.cuda.current_stream(t.device).cuda_stream
+
+
+def require_cuda(*tensors: torch.Tensor) -> None:
+    for t in tensors:
+        if not isinstance(t, torch.Tensor) or not t.is_cuda:
+            raise GPAWB200Error('gpaw_b200 operators take CUDA torch tensors '
+                                '(there is no CPU path)')
+        if not t.is_contiguous():
+            raise GPAWB200Error('arrays must be C-contiguous')
+
+
+def ptr(t: torch.Tensor) -> int:
+    return t.data_ptr()

@@ -1,0 +1,53 @@
+// Internal (non-ABI) declarations shared by the .cu files of libgpawb200.
+#pragma once
+#include <vector>
+#include "common.cuh"
+
+namespace gb {
+static constexpr int HMAX = 6;   // largest axis radius handled by star_kernel
+
+// out = alpha * Op(in) + beta * in + gamma * y   (y may be null)
+struct Epilogue {
+  double alpha = 1.0, beta = 0.0, gamma = 0.0;
+  const void* y = nullptr;
+};
+
+}  // namespace gb
+
+// operator object
+struct gb_operator {
+  int np;
+  std::vector<double> coef;
+  std::vector<int> off;    // np x 3
+  int64_t n[3];
+  int range;
+  int pbc[3];
+  int real;
+  int cfd;                 // all offsets on axes -> star kernel
+  int H;                   // largest axis offset
+  double center;
+  double a[3][2 * gb::HMAX + 1];
+  double diag;
+};
+
+
+struct gb_transformer {
+  int64_t nin_c[3], nout_c[3];
+  int k;              // 2 * nn
+  int interpolate;
+  int real;
+  int pbc[3];
+  // restriction: fine centre of coarse i is 2 i + off[c];
+  // interpolation: fine local f has global parity f + skip0[c], coarse local
+  // index of fine global F (even) is F/2 - cbeg[c]
+  int off[3];
+  int skip0[3], skip1[3];
+  int cbeg[3];
+};
+
+namespace gb {
+int op_apply(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype,
+             const double* ph, cudaStream_t st, const Epilogue& ep);
+int tr_apply(const gb_transformer* t, const void* in, void* out, int64_t nin, int dtype,
+             const double* ph, cudaStream_t st, double alpha, const void* y, double gamma);
+}  // namespace gb

@@ -1,0 +1,121 @@
+/*
+ * gpawb200.h -- C ABI of libgpawb200.so, the B200 (sm_100a) implementation of
+ * GPAW's real-space finite-difference Kohn-Sham hot path.
+ *
+ * Every entry point:
+ *   - takes plain pointers (device pointers for grid data), sizes and an
+ *     opaque cudaStream_t passed as void* (NULL = legacy default stream);
+ *   - returns an int status: GB_OK (0) or a negative GB_E* code, with a
+ *     message available from gb_last_error() (per host thread);
+ *   - never allocates its outputs: callers own every input/output buffer
+ *     (the reference's ownership rule, c/_gpaw.h objects borrow caller arrays).
+ *
+ * Grid arrays are C-contiguous (nbatch, n0, n1, n2) of one of the GB_DTYPE_*
+ * element types; complex arrays are interleaved (re, im).
+ *
+ * Each declaration cites the reference interface it replaces
+ * (path:line inside the GPAW source tree).
+ */
+#ifndef GPAWB200_H
+#define GPAWB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GB_OK               0
+#define GB_E_INVALID       -1   /* bad argument: shape, dtype, null pointer   */
+#define GB_E_UNSUPPORTED   -2   /* valid request this build does not handle   */
+#define GB_E_CUDA          -3   /* CUDA runtime/launch error                  */
+#define GB_E_NOMEM         -4   /* host/device allocation for an object failed */
+#define GB_E_TIMEOUT       -5   /* a bounded device-side wait gave up          */
+
+/* ---- element types ----------------------------------------------------- */
+#define GB_DTYPE_F64   0   /* double                        (numpy float)      */
+#define GB_DTYPE_F32   1   /* float                         (FP32 batched form) */
+#define GB_DTYPE_C128  2   /* double complex, interleaved   (numpy complex)    */
+#define GB_DTYPE_C64   3   /* float complex, interleaved                      */
+
+/* Message for the last failing call on this host thread ("" if none). */
+const char* gb_last_error(void);
+/* Library version string. */
+const char* gb_version(void);
+/* Number of SMs of the current device (used by the host-side autotuner). */
+int gb_device_sm_count(int* sm_count);
+
+/* ======================================================================
+ * FD operator (stencil)  -- replaces _gpaw.Operator
+ *   reference: c/operators.c:384-425 (NewOperatorObject),
+ *              c/operators.c:250-321 (Operator_apply),
+ *              c/operators.c:324-337 (get_diagonal_element),
+ *              c/bmgs/fd.c:9-33 (bmgs_fd), c/bc.c:146-308 (halo / BCs)
+ * ==================================================================== */
+typedef struct gb_operator gb_operator;
+
+/* coef_p[np], offset_p[np]: linear offsets in the array padded by `range`
+ * on each side (offset = o0*M1*M2 + o1*M2 + o2, M = n + 2*range), exactly
+ * as gpaw/fd_operators.py:55-57 builds them.  neighbor_cd[3][2]: -1 = zero
+ * boundary on that side, >= 0 = periodic (single domain).  `real` selects
+ * float vs complex data; `cfd` is the reference's central-FD flag (all
+ * offsets on the axes). */
+int gb_operator_new(const double* coef_p, const int64_t* offset_p, int np,
+                    const int64_t size_c[3], int range,
+                    const int64_t neighbor_cd[6], int real, int cfd,
+                    gb_operator** out);
+/* out = stencil(in) for nin stacked grids.  phase_cd: 3x2 complex Bloch
+ * phases as 12 doubles (re, im), required for complex dtypes, ignored for
+ * real ones (c/operators.c:270-273). */
+int gb_operator_apply(const gb_operator* op, const void* in, void* out,
+                      int64_t nin, int dtype, const double* phase_cd,
+                      void* stream);
+/* Weighted-Jacobi relaxation sweeps (relax_method 2) used by the FD Poisson
+ * solver: c/operators.c:55-97, c/bmgs/relax.c:7-66.  Real FP64 only. */
+int gb_operator_relax(const gb_operator* op, int relax_method, double* f_g,
+                      const double* s_g, int nrelax, double w, void* stream);
+int gb_operator_get_diagonal_element(const gb_operator* op, double* d);
+int gb_operator_free(gb_operator* op);
+
+/* ======================================================================
+ * Transformer (restriction / interpolation)  -- replaces _gpaw.Transformer
+ *   reference: c/transformers.c:202-252 (NewTransformerObject),
+ *              c/transformers.c:44-164 (apply), c/bmgs/restrict.c:136-155,
+ *              c/bmgs/interpolate.c:227-257, gpaw/transformers.py:27-77
+ * ==================================================================== */
+typedef struct gb_transformer gb_transformer;
+
+/* Arguments as in gpaw/transformers.py:71-77: size_in/size_out = gdin.n_c /
+ * gdout.n_c, k = 2*nn (2, 4, 6, 8), pad_cd/npad_cd/skip_cd [3][2],
+ * neighbor_cd [3][2] of the input grid, interpolate = 0 (restrict) / 1. */
+int gb_transformer_new(const int64_t size_in[3], const int64_t size_out[3],
+                       int k, const int64_t pad_cd[6], const int64_t npad_cd[6],
+                       const int64_t skip_cd[6], const int64_t neighbor_cd[6],
+                       int real, int interpolate, gb_transformer** out);
+int gb_transformer_apply(const gb_transformer* t, const void* in, void* out,
+                         int64_t nin, int dtype, const double* phase_cd,
+                         void* stream);
+int gb_transformer_free(gb_transformer* t);
+
+/* ======================================================================
+ * Multigrid preconditioner V-cycle  -- replaces _gpaw.fd_precond
+ *   reference: c/fd_preconditioner.c:108-353, gpaw/preconditioner.py:59-93
+ * Work arrays as in the reference: d0,q0 (nin, level-0 grid); r1,d1,q1
+ * (nin, level-1); r2,d2,q2 (nin, level-2).  The result is written to d0.
+ * nresiduals may be NULL (the negation is done on the fly).
+ * ==================================================================== */
+int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* rest1,
+                  const gb_transformer* intp1, const gb_transformer* intp2,
+                  const gb_operator* kin0, const gb_operator* kin1,
+                  const gb_operator* kin2,
+                  void* d0, void* q0, void* r1, void* d1, void* q1,
+                  void* r2, void* d2, void* q2,
+                  const void* residuals, const void* nresiduals,
+                  double step, int64_t nin, int dtype,
+                  const double* phase_cd, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPAWB200_H */

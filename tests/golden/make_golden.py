@@ -1,0 +1,192 @@
+"""Generate the golden vectors under tests/golden/ from the reference itself.
+
+Run in a container that has the reference source tree (REF, default
+/root/reference) and GPAW's C extension built from it by oracle/Makefile:
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Outputs (committed; read by the CPU and GPU tests, which never need the
+reference tree at run time):
+  stencils.json  coefficient / offset lists of the reference's
+                 gpaw.fd_operators.Laplace / Gradient for a set of cells
+  fd_kernels.npz outputs of _gpaw.Operator / Transformer / fd_precond on
+                 seeded inputs (numpy default_rng(seed).standard_normal, so
+                 inputs are regenerated from the seed, not stored)
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+REF = os.environ.get('REF', '/root/reference')
+sys.path.insert(0, str(REPO / 'oracle' / '_ref'))
+sys.path.insert(1, REF)
+sys.path.insert(2, str(REPO))
+sys.path.insert(3, str(HERE))
+
+import _gpaw  # noqa: E402  (the reference C extension built from source)
+import gpaw.fd_operators as ref_fd  # noqa: E402
+from oracle import ref as oref  # noqa: E402
+from oracle.fd import transformer_geometry  # noqa: E402
+
+from cells import CELLS  # noqa: E402
+
+
+class StubComm:
+    size = 1
+    rank = 0
+
+    def get_c_object(self):
+        return None
+
+
+class StubGD:
+    """The attributes gpaw.fd_operators reads from a GridDescriptor."""
+
+    def __init__(self, N_c, cell, pbc):
+        cell = np.array(cell, float)
+        self.cell_cv = np.diag(cell) if cell.ndim == 1 else cell
+        self.N_c = np.array(N_c)
+        self.pbc_c = np.array(pbc, bool)
+        self.beg_c = np.where(self.pbc_c, 0, 1)
+        self.n_c = self.N_c - self.beg_c
+        self.h_cv = self.cell_cv / self.N_c[:, None]
+        self.neighbor_cd = np.ascontiguousarray(
+            np.where(self.pbc_c[:, None], 0, -1) * np.ones((3, 2), int))
+        self.comm = StubComm()
+
+
+def stencils():
+    out = {}
+    for name, cell in CELLS.items():
+        gd = StubGD((12, 12, 12), cell, (1, 1, 1))
+        for n in (1, 2, 3, 4):
+            lap = ref_fd.Laplace(gd, -0.5, n)
+            out[f'laplace/{name}/{n}'] = {
+                'coef': lap.coef_p.tolist(),
+                'offset': np.asarray(lap.offset_pc).tolist()}
+            for v in range(3):
+                g = ref_fd.Gradient(gd, v, 1.0, n)
+                out[f'gradient/{name}/{n}/{v}'] = {
+                    'coef': np.asarray(g.coef_p).tolist(),
+                    'offset': np.asarray(g.offset_pc).tolist()}
+    return out
+
+
+def phases(pbc, k_c):
+    sd = np.zeros((3, 2))
+    p = np.asarray(pbc, bool)
+    sd[p, 0] = 1
+    sd[p, 1] = -1
+    return np.exp(2j * np.pi * sd * np.asarray(k_c)[:, None])
+
+
+def seeded(seed, shape, cplx):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal(shape)
+    if cplx:
+        a = a + 1j * rng.standard_normal(shape)
+    return a
+
+
+K_C = (0.1, 0.25, -0.3)
+N_KERNEL = (6, 7, 8)
+
+
+def kernels(sten):
+    res = {}
+    seed = 100
+    # stencils: orthorhombic Laplace nn=1..3, GUC (hexagonal, fcc) n=2, gradients
+    cases = [('laplace/ortho/3', 'ortho'), ('laplace/ortho/1', 'ortho'),
+             ('laplace/ortho/2', 'ortho'), ('laplace/hexagonal/2', 'hexagonal'),
+             ('laplace/fcc/2', 'fcc'), ('gradient/ortho/3/0', 'ortho'),
+             ('gradient/ortho/3/2', 'ortho'), ('gradient/hexagonal/2/1', 'hexagonal')]
+    for key, _ in cases:
+        st = sten[key]
+        for pbc in ((0, 0, 0), (1, 1, 1), (1, 0, 1)):
+            for cplx in (False, True):
+                seed += 1
+                n_c = np.array(N_KERNEL) - (1 - np.array(pbc))
+                a = seeded(seed, (1,) + tuple(n_c), cplx)
+                op = oref.operator(st['coef'], st['offset'], n_c, pbc, not cplx)
+                b = np.zeros_like(a)
+                if cplx:
+                    op.apply(a, b, phases(pbc, K_C))
+                else:
+                    op.apply(a, b)
+                res[f'op|{key}|{"".join(map(str, pbc))}|{int(cplx)}|{seed}'] = b
+    # transformers: restrict / interpolate, k = 2..8
+    # (grids large enough for the reference's own "Cannot construct
+    # interpolator" rule, gpaw/transformers.py:49-55; smaller ones are invalid)
+    for pbc in ((0, 0, 0), (1, 1, 1)):
+        N = np.array((16, 16, 20))
+        beg_f = np.where(pbc, 0, 1)
+        for nn in (1, 2, 3, 4):
+            for cplx in ((False, True) if nn in (1, 3) else (False,)):
+                for restrict in (True, False):
+                    seed += 1
+                    Nin = N if restrict else N // 2
+                    Nout = N // 2 if restrict else N
+                    beg_in = beg_f
+                    beg_out = beg_f
+                    pad, npad, skip = transformer_geometry(
+                        beg_in, Nin, beg_out, Nout, nn, restrict)
+                    n_in = Nin - beg_in
+                    n_out = Nout - beg_out
+                    t = oref.transformer(n_in, n_out, nn, pad, npad, skip, pbc,
+                                         not cplx, not restrict)
+                    a = seeded(seed, (1,) + tuple(n_in), cplx)
+                    b = np.zeros((1,) + tuple(n_out), a.dtype)
+                    if cplx:
+                        t.apply(a, b, phases(pbc, K_C))
+                    else:
+                        t.apply(a, b)
+                    res[f'tr|{"".join(map(str, pbc))}|{nn}|{int(cplx)}|'
+                        f'{"R" if restrict else "I"}|{seed}'] = b
+    # multigrid preconditioner
+    for pbc, cplx in (((0, 0, 0), False), ((1, 1, 1), False), ((1, 1, 1), True)):
+        seed += 1
+        N0 = np.array((12, 12, 16))
+        cell = np.array([3.2, 3.2, 4.0])
+        gds = [StubGD(N0 // 2**lvl, cell, pbc) for lvl in range(3)]
+        kin = [ref_fd.Laplace(gds[0], -0.5, 3, float if not cplx else complex)]
+        kin += [ref_fd.Laplace(g, -0.5, 1, float if not cplx else complex) for g in gds[1:]]
+        ops = [k.operator for k in kin]
+
+        def T(gi, go):
+            r = (gi.N_c == 2 * go.N_c).all()
+            pad, npad, skip = transformer_geometry(gi.beg_c, gi.N_c, go.beg_c, go.N_c, 1, r)
+            return oref.transformer(gi.n_c, go.n_c, 1, pad, npad, skip, pbc, not cplx, not r)
+
+        rest0, rest1 = T(gds[0], gds[1]), T(gds[1], gds[2])
+        intp2, intp1 = T(gds[2], gds[1]), T(gds[1], gds[0])
+        B = 2
+        dt = complex if cplx else float
+        R = seeded(seed, (B,) + tuple(gds[0].n_c), cplx).astype(dt)
+        d0 = np.zeros_like(R)
+        q0 = np.zeros_like(R)
+        w1 = [np.zeros((B,) + tuple(gds[1].n_c), dt) for _ in range(3)]
+        w2 = [np.zeros((B,) + tuple(gds[2].n_c), dt) for _ in range(3)]
+        step = 0.66666666 / kin[0].get_diagonal_element()
+        _gpaw.fd_precond(rest0, rest1, intp1, intp2, *ops, d0, q0, *w1, *w2,
+                         R, -R, step, phases(pbc, K_C))
+        res[f'pc|{"".join(map(str, pbc))}|{int(cplx)}|{seed}'] = d0
+    return res
+
+
+def main():
+    sten = stencils()
+    (HERE / 'stencils.json').write_text(json.dumps(sten))
+    res = kernels(sten)
+    np.savez_compressed(HERE / 'fd_kernels.npz', **res)
+    print(f'{len(sten)} stencils, {len(res)} kernel outputs')
+
+
+if __name__ == '__main__':
+    main()
