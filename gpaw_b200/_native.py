@@ -45,6 +45,8 @@ _SIGNATURES = {
     'gb_transformer_apply': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,
                                      c_int, PD, c_void_p]),
     'gb_transformer_free': (c_int, [c_void_p]),
+    'gb_xc_calculate': (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p,
+                                c_void_p, c_void_p, c_void_p, c_void_p]),
     'gb_fd_precond': (c_int, [c_void_p] * 7 + [c_void_p] * 8 +
                       [c_void_p, c_void_p, c_double, c_int64, c_int, PD,
                        c_void_p]),

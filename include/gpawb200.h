@@ -115,6 +115,20 @@ int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* rest1,
                   double step, int64_t nin, int dtype,
                   const double* phase_cd, void* stream);
 
+/* ======================================================================
+ * Exchange-correlation on the grid  -- replaces _gpaw.XCFunctional.calculate
+ *   reference: c/xc/xc.c:73-227 (spin-paired / polarised drivers),
+ *              c/xc/pbe.c (PBE exchange + PW92/PBE correlation),
+ *              c/xc/rpbe.c, gpaw/xc/kernel.py:6-58 (codes)
+ * code: -1 LDA, 0 PBE, 1 revPBE, 2 RPBE.  FP64 device arrays of ng points:
+ * e_g [ng] (overwritten), n_sg [nspins][ng], v_sg [nspins][ng] (ADDED to,
+ * as in the reference), sigma_xg / dedsigma_xg [2*nspins-1][ng] (GGA only;
+ * dedsigma overwritten).
+ * ==================================================================== */
+int gb_xc_calculate(int code, int nspins, int64_t ng, double* e_g,
+                    const double* n_sg, double* v_sg, const double* sigma_xg,
+                    double* dedsigma_xg, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -180,7 +180,30 @@ def kernels(sten):
     return res
 
 
+def xc_golden():
+    from oracle.xc import log_uniform_inputs
+    res = {}
+    for code in (-1, 0, 1, 2):
+        for nspins in (1, 2):
+            n_sg, sigma_xg = log_uniform_inputs(1000 + 10 * code + nspins, nspins, 1000)
+            e_g = np.zeros(n_sg.shape[1])
+            v_sg = np.zeros_like(n_sg)
+            dedsigma_xg = np.zeros_like(sigma_xg)
+            X = _gpaw.XCFunctional(code)
+            if code == -1:
+                X.calculate(e_g, n_sg, v_sg)
+            else:
+                X.calculate(e_g, n_sg, v_sg, sigma_xg, dedsigma_xg)
+            key = f'{code}|{nspins}'
+            res[f'e|{key}'] = e_g
+            res[f'v|{key}'] = v_sg
+            if code != -1:
+                res[f'dedsigma|{key}'] = dedsigma_xg
+    return res
+
+
 def main():
+    np.savez_compressed(HERE / 'xc.npz', **xc_golden())
     sten = stencils()
     (HERE / 'stencils.json').write_text(json.dumps(sten))
     res = kernels(sten)

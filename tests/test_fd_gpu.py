@@ -208,7 +208,7 @@ def test_empty_batch_and_errors():
                   torch.zeros((8, 8, 8), dtype=torch.complex128, device='cuda'))
     with pytest.raises(nat.GPAWB200Error):
         lap.apply(torch.zeros((8, 8, 8), dtype=torch.float64, device='cuda'),
-                  torch.zeros((8, 8, 8), dtype=torch.float64, device='cuda').t())
+                  torch.zeros((8, 8, 16), dtype=torch.float64, device='cuda')[:, :, ::2])
 
 
 @pytest.mark.parametrize('dtype,pbc', [(torch.float64, (1, 1, 1)),
