@@ -1,0 +1,453 @@
+// Localized functions: add / integrate (replaces _gpaw.LFC: c/lfc.c:146-257
+// NewLFCObject, 432-505 integrate, 818-885 add, c/lfc.h:79-130 GRID_LOOP).
+//
+// The reference walks the merged, sorted list of sphere boundaries once per
+// band on one core.  Here the same sweep runs once, on the host, when the
+// object is built (positions change rarely), and produces two device-side
+// indexings of the (grid point, volume, row) incidence:
+//
+//  * point-major (add):  every grid point covered by at least one sphere owns
+//    one thread; it sums  sum_W conj(phase_W) sum_m A_W[row][m] c[x][M_W + m]
+//    over the volumes covering it and adds to a[x][G] -- every a[x][G] has a
+//    single writer, so there are no atomics and results are deterministic.
+//  * function-group-major (integrate): a group is one (atom, radial function)
+//    M-range with all its periodic images; one CTA per (group, band block)
+//    reduces dv * phase_W * sum_G a[x][G] A_W[row][m] over every image and
+//    adds the block's result to c[x][M..M+nm) -- again a single writer.
+//
+// Derivatives (forces) use the same integrate kernel on a second object whose
+// rows hold the 3*nm Cartesian derivatives (layout [m][v], c_xMv).
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <type_traits>
+#include <vector>
+#include "internal.cuh"
+
+struct gb_lfc {
+  int nW = 0, nM = 0, maxnm = 0;
+  int64_t nG = 0;
+  double dv = 1.0;
+  int nq = 0;
+  // device data
+  double* A64 = nullptr;      // concatenated rows of every volume
+  float* A32 = nullptr;
+  int64_t nA = 0;             // doubles in A
+  double2* phase = nullptr;   // [nq][nW]
+  // add (point-major)
+  int64_t P = 0;              // covered points
+  int* pt_G = nullptr;        // [P]
+  int* pt_off = nullptr;      // [P+1] into contributions
+  int64_t C = 0;              // contributions
+  int64_t* ct_aoff = nullptr; // [C] offset into A (doubles)
+  int* ct_M = nullptr;        // [C]
+  int* ct_nm = nullptr;       // [C]
+  int* ct_W = nullptr;        // [C]
+  // integrate (group-major)
+  int ngroups = 0;
+  int* gr_M = nullptr;        // [ngroups]
+  int* gr_nm = nullptr;       // [ngroups]
+  int* gr_voff = nullptr;     // [ngroups+1] into the volume list
+  int* gv_W = nullptr;        // [nW] volumes ordered by group
+  int64_t* vol_row0 = nullptr;  // [nW] first global row of W
+  int64_t* vol_row1 = nullptr;  // [nW] one past last
+  int* row_G = nullptr;       // [rows] grid point of every global row
+  int64_t* vol_aoff = nullptr;  // [nW] offset (doubles) of row0 in A
+  std::vector<int> h_gr_nm;
+  std::vector<void*> allocations;
+};
+
+namespace gb {
+
+// trivially-copyable device view passed to the kernels
+struct LfcView {
+  int nW, nM;
+  int64_t nG;
+  double dv;
+  const double2* phase;
+  int64_t P;
+  const int* pt_G;
+  const int* pt_off;
+  const int64_t* ct_aoff;
+  const int* ct_M;
+  const int* ct_nm;
+  const int* ct_W;
+  const int* gr_M;
+  const int* gr_voff;
+  const int* gv_W;
+  const int64_t* vol_row0;
+  const int64_t* vol_row1;
+  const int* row_G;
+  const int64_t* vol_aoff;
+};
+
+static LfcView view(const gb_lfc* l) {
+  LfcView v;
+  v.nW = l->nW; v.nM = l->nM; v.nG = l->nG; v.dv = l->dv; v.phase = l->phase;
+  v.P = l->P; v.pt_G = l->pt_G; v.pt_off = l->pt_off; v.ct_aoff = l->ct_aoff;
+  v.ct_M = l->ct_M; v.ct_nm = l->ct_nm; v.ct_W = l->ct_W; v.gr_M = l->gr_M;
+  v.gr_voff = l->gr_voff; v.gv_W = l->gv_W; v.vol_row0 = l->vol_row0;
+  v.vol_row1 = l->vol_row1; v.row_G = l->row_G; v.vol_aoff = l->vol_aoff;
+  return v;
+}
+
+template <typename T>
+static T* dalloc(gb_lfc* l, size_t n) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+  l->allocations.push_back(p);
+  return reinterpret_cast<T*>(p);
+}
+
+template <typename T>
+static bool upload(gb_lfc* l, T** dst, const std::vector<T>& src) {
+  *dst = dalloc<T>(l, src.size());
+  if (!*dst) return false;
+  if (!src.empty() && cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return false;
+  return true;
+}
+
+// --------------------------------------------------------------------- add
+template <typename T> struct AType { using A = double; };
+template <> struct AType<float> { using A = float; };
+template <> struct AType<float2> { using A = float; };
+
+template <typename T, int XB>
+__global__ void lfc_add_kernel(const LfcView l, const typename AType<T>::A* __restrict__ A,
+                               const T* __restrict__ c_xM, T* __restrict__ a_xG, int64_t nx, int q) {
+  using R = typename Elem<T>::R;
+  constexpr bool CPLX = Elem<T>::cplx;
+  const int64_t x0 = (int64_t)blockIdx.y * XB;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < l.P; p += (int64_t)gridDim.x * blockDim.x) {
+    const int G = l.pt_G[p];
+    T acc[XB];
+#pragma unroll
+    for (int i = 0; i < XB; ++i) acc[i] = zero<T>();
+    const int c1 = l.pt_off[p + 1];
+    for (int c = l.pt_off[p]; c < c1; ++c) {
+      const typename AType<T>::A* Ar = A + l.ct_aoff[c];
+      const int M = l.ct_M[c], nm = l.ct_nm[c];
+      double pr = 1.0, pi = 0.0;
+      if (CPLX && q >= 0) {
+        const double2 ph = l.phase[(int64_t)q * l.nW + l.ct_W[c]];
+        pr = ph.x; pi = -ph.y;   // conj(phase) (c/lfc.c:864)
+      }
+#pragma unroll
+      for (int i = 0; i < XB; ++i) {
+        if (x0 + i >= nx) break;
+        const T* cx = c_xM + (x0 + i) * l.nM + M;
+        T s = zero<T>();
+        for (int m = 0; m < nm; ++m) s = fmadd(s, (R)Ar[m], cx[m]);
+        acc[i] = add(acc[i], CPLX ? phase_mul(s, pr, pi) : s);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < XB; ++i) {
+      if (x0 + i >= nx) break;
+      T* ap = a_xG + (x0 + i) * l.nG + G;
+      *ap = add(*ap, acc[i]);
+    }
+  }
+}
+
+// --------------------------------------------------------------- integrate
+template <typename T, int NM, int XB, int NT>
+__global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, const typename AType<T>::A* __restrict__ A,
+                                                          const T* __restrict__ a_xG, T* __restrict__ c_xM,
+                                                          int64_t nx, int q, int group_base) {
+  using R = typename Elem<T>::R;
+  constexpr bool CPLX = Elem<T>::cplx;
+  __shared__ T red[NT / 32][XB * NM];
+  const int g = group_base + blockIdx.x;
+  const int64_t x0 = (int64_t)blockIdx.y * XB;
+  const int M = l.gr_M[g];
+  T acc[XB][NM];
+#pragma unroll
+  for (int i = 0; i < XB; ++i)
+#pragma unroll
+    for (int m = 0; m < NM; ++m) acc[i][m] = zero<T>();
+  for (int vi = l.gr_voff[g]; vi < l.gr_voff[g + 1]; ++vi) {
+    const int W = l.gv_W[vi];
+    const int64_t r0 = l.vol_row0[W], r1 = l.vol_row1[W];
+    const typename AType<T>::A* AW = A + l.vol_aoff[W];
+    double pr = 1.0, pi = 0.0;
+    if (CPLX && q >= 0) {
+      const double2 ph = l.phase[(int64_t)q * l.nW + W];
+      pr = ph.x; pi = ph.y;
+    }
+    T part[XB][NM];
+#pragma unroll
+    for (int i = 0; i < XB; ++i)
+#pragma unroll
+      for (int m = 0; m < NM; ++m) part[i][m] = zero<T>();
+    for (int64_t r = r0 + threadIdx.x; r < r1; r += NT) {
+      const int G = l.row_G[r];
+      R Ar[NM];
+#pragma unroll
+      for (int m = 0; m < NM; ++m) Ar[m] = (R)AW[(r - r0) * NM + m];
+#pragma unroll
+      for (int i = 0; i < XB; ++i) {
+        if (x0 + i >= nx) break;
+        const T v = a_xG[(x0 + i) * l.nG + G];
+#pragma unroll
+        for (int m = 0; m < NM; ++m) part[i][m] = fmadd(part[i][m], Ar[m], v);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < XB; ++i)
+#pragma unroll
+      for (int m = 0; m < NM; ++m) acc[i][m] = add(acc[i][m], CPLX ? phase_mul(part[i][m], pr, pi) : part[i][m]);
+  }
+  // block reduction: warp shuffles, then across warps
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < XB; ++i)
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+      T v = acc[i][m];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        if constexpr (CPLX) {
+          v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+          v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+        } else {
+          v += __shfl_down_sync(0xffffffffu, v, o);
+        }
+      }
+      if (lane == 0) red[warp][i * NM + m] = v;
+    }
+  __syncthreads();
+  for (int e = threadIdx.x; e < XB * NM; e += NT) {
+    const int i = e / NM, m = e % NM;
+    if (x0 + i >= nx) continue;
+    T v = zero<T>();
+    for (int w = 0; w < NT / 32; ++w) v = add(v, red[w][e]);
+    T* cp = c_xM + (x0 + i) * l.nM + M + m;
+    *cp = fmadd(*cp, (R)l.dv, v);
+  }
+}
+
+template <typename T, int NM>
+static int integrate_nm(const gb_lfc* l, int gbeg, int gcount, const void* a, void* c, int64_t nx, int q,
+                        cudaStream_t st) {
+  constexpr int XB = NM <= 3 ? 8 : (NM <= 9 ? 4 : 2);
+  constexpr int NT = 128;
+  const typename AType<T>::A* A;
+  if constexpr (std::is_same<typename AType<T>::A, float>::value) A = l->A32; else A = l->A64;
+  dim3 grid((unsigned)gcount, (unsigned)((nx + XB - 1) / XB));
+  lfc_integrate_kernel<T, NM, XB, NT><<<grid, NT, 0, st>>>(view(l), A, (const T*)a, (T*)c, nx, q, gbeg);
+  return check_launch("lfc_integrate_kernel");
+}
+
+template <typename T>
+static int integrate_t(const gb_lfc* l, const void* a, void* c, int64_t nx, int q, cudaStream_t st) {
+  // groups are sorted by nm on the host; launch one kernel per nm class
+  int g = 0;
+  while (g < l->ngroups) {
+    const int nm = l->h_gr_nm[g];
+    int e = g;
+    while (e < l->ngroups && l->h_gr_nm[e] == nm) ++e;
+    int rc;
+    switch (nm) {
+      case 1: rc = integrate_nm<T, 1>(l, g, e - g, a, c, nx, q, st); break;
+      case 3: rc = integrate_nm<T, 3>(l, g, e - g, a, c, nx, q, st); break;
+      case 5: rc = integrate_nm<T, 5>(l, g, e - g, a, c, nx, q, st); break;
+      case 7: rc = integrate_nm<T, 7>(l, g, e - g, a, c, nx, q, st); break;
+      case 9: rc = integrate_nm<T, 9>(l, g, e - g, a, c, nx, q, st); break;
+      case 15: rc = integrate_nm<T, 15>(l, g, e - g, a, c, nx, q, st); break;
+      case 21: rc = integrate_nm<T, 21>(l, g, e - g, a, c, nx, q, st); break;
+      case 27: rc = integrate_nm<T, 27>(l, g, e - g, a, c, nx, q, st); break;
+      default: return fail(GB_E_UNSUPPORTED, "lfc: function count per radial function not in {1,3,5,7,9,15,21,27}");
+    }
+    if (rc) return rc;
+    g = e;
+  }
+  return GB_OK;
+}
+
+template <typename T>
+static int add_t(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st) {
+  constexpr int XB = 8;
+  if (l->P == 0) return GB_OK;
+  const typename AType<T>::A* A;
+  if constexpr (std::is_same<typename AType<T>::A, float>::value) A = l->A32; else A = l->A64;
+  const int NT = 256;
+  const int64_t bx = std::min<int64_t>((l->P + NT - 1) / NT, (int64_t)sm_count() * 8);
+  dim3 grid((unsigned)bx, (unsigned)((nx + XB - 1) / XB));
+  lfc_add_kernel<T, XB><<<grid, NT, 0, st>>>(view(l), A, (const T*)c, (T*)a, nx, q);
+  return check_launch("lfc_add_kernel");
+}
+
+static __global__ void to_float(const double* a, float* b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+}  // namespace gb
+
+using namespace gb;
+
+extern "C" {
+
+int gb_lfc_free(gb_lfc* l) {
+  if (!l) return GB_OK;
+  for (void* p : l->allocations) cudaFree(p);
+  delete l;
+  return GB_OK;
+}
+
+int gb_lfc_new(int nW, const double* A_all, const int64_t* ngm_W, const int* nm_W, const int* M_W, int nB,
+               const int* G_B, const int* W_B, double dv, int nq, const double* phase_qW, int64_t nG, int nM,
+               gb_lfc** out) {
+  GB_REQUIRE(out && nW >= 0 && nB >= 0 && nG > 0 && nM >= 0, "gb_lfc_new: bad arguments");
+  GB_REQUIRE(nW == 0 || (A_all && ngm_W && nm_W && M_W && G_B && W_B), "gb_lfc_new: null pointer");
+  GB_REQUIRE(nq == 0 || phase_qW, "gb_lfc_new: phases missing");
+  GB_REQUIRE(nG < (int64_t)1 << 31, "gb_lfc_new: grid too large for 32-bit point indices");
+  auto* l = new (std::nothrow) gb_lfc();
+  if (!l) return fail(GB_E_NOMEM, "gb_lfc_new: out of host memory");
+  l->nW = nW; l->nG = nG; l->nM = nM; l->dv = dv; l->nq = nq;
+  // global row / A offsets per volume
+  std::vector<int64_t> row0(nW + 1, 0), aoff(nW + 1, 0);
+  for (int W = 0; W < nW; ++W) {
+    if (nm_W[W] < 1 || ngm_W[W] < 0 || M_W[W] < 0 || M_W[W] + nm_W[W] > nM) {
+      gb_lfc_free(l);
+      return fail(GB_E_INVALID, "gb_lfc_new: bad volume description");
+    }
+    row0[W + 1] = row0[W] + ngm_W[W];
+    aoff[W + 1] = aoff[W] + ngm_W[W] * nm_W[W];
+    l->maxnm = std::max(l->maxnm, nm_W[W]);
+  }
+  // GRID_LOOP sweep (c/lfc.h:79-130): the rows of a volume are consumed in
+  // increasing G over the runs in which it is current.
+  std::vector<int> row_G(row0[nW]);
+  std::vector<int64_t> next_row(row0.begin(), row0.end() - 1);
+  std::vector<int> cur;                 // current volumes
+  std::vector<int> pos_in_cur(nW, -1);
+  std::vector<int> pt_G, pt_off(1, 0);
+  std::vector<int64_t> ct_aoff;
+  std::vector<int> ct_M, ct_nm, ct_W;
+  int Ga = 0;
+  for (int B = 0; B < nB; ++B) {
+    const int Gb = G_B[B];
+    if (Gb < Ga || Gb > nG) {
+      gb_lfc_free(l);
+      return fail(GB_E_INVALID, "gb_lfc_new: boundary list not sorted or out of range");
+    }
+    if (Gb > Ga && !cur.empty()) {
+      for (int G = Ga; G < Gb; ++G) {
+        pt_G.push_back(G);
+        for (int W : cur) {
+          const int64_t r = next_row[W]++;
+          if (r >= row0[W + 1]) {
+            gb_lfc_free(l);
+            return fail(GB_E_INVALID, "gb_lfc_new: boundaries cover more points than a volume has rows");
+          }
+          row_G[r] = G;
+          ct_aoff.push_back(aoff[W] + (r - row0[W]) * nm_W[W]);
+          ct_M.push_back(M_W[W]);
+          ct_nm.push_back(nm_W[W]);
+          ct_W.push_back(W);
+        }
+        pt_off.push_back((int)ct_W.size());
+      }
+    }
+    const int Wn = W_B[B];
+    if (Wn >= 0) {
+      if (Wn >= nW || pos_in_cur[Wn] >= 0) {
+        gb_lfc_free(l);
+        return fail(GB_E_INVALID, "gb_lfc_new: bad volume entry");
+      }
+      pos_in_cur[Wn] = (int)cur.size();
+      cur.push_back(Wn);
+    } else {
+      const int Wo = -1 - Wn;
+      if (Wo >= nW || pos_in_cur[Wo] < 0) {
+        gb_lfc_free(l);
+        return fail(GB_E_INVALID, "gb_lfc_new: volume leaves before entering");
+      }
+      const int i = pos_in_cur[Wo];
+      cur[i] = cur.back();
+      pos_in_cur[cur[i]] = i;
+      cur.pop_back();
+      pos_in_cur[Wo] = -1;
+    }
+    Ga = Gb;
+  }
+  for (int W = 0; W < nW; ++W)
+    if (next_row[W] != row0[W + 1]) {
+      gb_lfc_free(l);
+      return fail(GB_E_INVALID, "gb_lfc_new: volume rows and boundary runs disagree");
+    }
+  // function groups: volumes sharing (M, nm), ordered by nm for per-class launches
+  std::map<std::pair<int, int>, std::vector<int>> groups;   // (nm, M) -> volumes
+  for (int W = 0; W < nW; ++W) groups[{nm_W[W], M_W[W]}].push_back(W);
+  std::vector<int> gr_M, gr_nm, gr_voff(1, 0), gv_W;
+  for (auto& kv : groups) {
+    gr_nm.push_back(kv.first.first);
+    gr_M.push_back(kv.first.second);
+    for (int W : kv.second) gv_W.push_back(W);
+    gr_voff.push_back((int)gv_W.size());
+  }
+  l->ngroups = (int)gr_M.size();
+  l->h_gr_nm = gr_nm;
+  l->P = (int64_t)pt_G.size();
+  l->C = (int64_t)ct_W.size();
+  l->nA = aoff[nW];
+  std::vector<int64_t> vr0(row0.begin(), row0.end() - 1), vr1(row0.begin() + 1, row0.end());
+  std::vector<int64_t> va(aoff.begin(), aoff.end() - 1);
+  std::vector<double> hA(A_all, A_all + l->nA);
+  std::vector<double2> ph;
+  for (int64_t i = 0; i < (int64_t)nq * nW; ++i) ph.push_back(make_double2(phase_qW[2 * i], phase_qW[2 * i + 1]));
+  bool ok = upload(l, &l->A64, hA) && upload(l, &l->pt_G, pt_G) && upload(l, &l->pt_off, pt_off) &&
+            upload(l, &l->ct_aoff, ct_aoff) && upload(l, &l->ct_M, ct_M) && upload(l, &l->ct_nm, ct_nm) &&
+            upload(l, &l->ct_W, ct_W) && upload(l, &l->gr_M, gr_M) && upload(l, &l->gr_nm, gr_nm) &&
+            upload(l, &l->gr_voff, gr_voff) && upload(l, &l->gv_W, gv_W) && upload(l, &l->vol_row0, vr0) &&
+            upload(l, &l->vol_row1, vr1) && upload(l, &l->row_G, row_G) && upload(l, &l->vol_aoff, va) &&
+            upload(l, &l->phase, ph);
+  if (ok) {
+    l->A32 = dalloc<float>(l, l->nA);
+    ok = l->A32 != nullptr;
+    if (ok && l->nA) {
+      to_float<<<std::min<int64_t>((l->nA + 255) / 256, 4096), 256>>>(l->A64, l->A32, l->nA);
+      ok = cudaDeviceSynchronize() == cudaSuccess;
+    }
+  }
+  if (!ok) {
+    gb_lfc_free(l);
+    return fail(GB_E_NOMEM, "gb_lfc_new: device allocation / upload failed");
+  }
+  *out = l;
+  return GB_OK;
+}
+
+int gb_lfc_add(const gb_lfc* l, const void* c_xM, void* a_xG, int64_t nx, int dtype, int q, void* stream) {
+  GB_REQUIRE(l && dtype_valid(dtype) && nx >= 0, "gb_lfc_add: bad arguments");
+  if (nx == 0) return GB_OK;
+  GB_REQUIRE(c_xM && a_xG, "gb_lfc_add: null array");
+  GB_REQUIRE(q < l->nq, "gb_lfc_add: k-point index out of range");
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (dtype) {
+    case GB_DTYPE_F64: return add_t<double>(l, c_xM, a_xG, nx, -1, st);
+    case GB_DTYPE_F32: return add_t<float>(l, c_xM, a_xG, nx, -1, st);
+    case GB_DTYPE_C128: return add_t<double2>(l, c_xM, a_xG, nx, q, st);
+    default: return add_t<float2>(l, c_xM, a_xG, nx, q, st);
+  }
+}
+
+int gb_lfc_integrate(const gb_lfc* l, const void* a_xG, void* c_xM, int64_t nx, int dtype, int q, void* stream) {
+  GB_REQUIRE(l && dtype_valid(dtype) && nx >= 0, "gb_lfc_integrate: bad arguments");
+  if (nx == 0) return GB_OK;
+  GB_REQUIRE(c_xM && a_xG, "gb_lfc_integrate: null array");
+  GB_REQUIRE(q < l->nq, "gb_lfc_integrate: k-point index out of range");
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (dtype) {
+    case GB_DTYPE_F64: return integrate_t<double>(l, a_xG, c_xM, nx, -1, st);
+    case GB_DTYPE_F32: return integrate_t<float>(l, a_xG, c_xM, nx, -1, st);
+    case GB_DTYPE_C128: return integrate_t<double2>(l, a_xG, c_xM, nx, q, st);
+    default: return integrate_t<float2>(l, a_xG, c_xM, nx, q, st);
+  }
+}
+
+}  // extern "C"

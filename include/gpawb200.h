@@ -116,6 +116,33 @@ int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* rest1,
                   const double* phase_cd, void* stream);
 
 /* ======================================================================
+ * Localized functions (LFC)  -- replaces _gpaw.LFC
+ *   reference: c/lfc.c:146-257 (NewLFCObject), c/lfc.c:818-885 (add),
+ *              c/lfc.c:432-505 (integrate), c/lfc.h:79-130 (GRID_LOOP),
+ *              gpaw/lfc.py:259-374 (_update builds the arguments)
+ * The arguments are the reference's, flattened to plain arrays (host
+ * memory): the nW volumes' A_gm blocks concatenated row-major in A_all
+ * (ngm_W[W] rows of nm_W[W] values each), M_W, the sorted boundary list
+ * G_B/W_B (W >= 0 enters volume W, -W-1 leaves it), dv, and phase_qW as
+ * nq*nW complex numbers (re, im) (nq = 0: Gamma point / real).  nG is the
+ * number of grid points per band, nM the length of c_xM rows.
+ * add:       a_xG[x] += sum_W conj(phase_qW) sum_m c_xM[x][M_W+m] A_W
+ * integrate: c_xM[x][M_W+m] += dv sum_G phase_qW a_xG[x][G] A_W[g][m]
+ *            (accumulates, like the reference; callers zero c_xM)
+ * q = -1 for real data / no Bloch phase.  Device arrays for a_xG / c_xM.
+ * ==================================================================== */
+typedef struct gb_lfc gb_lfc;
+int gb_lfc_new(int nW, const double* A_all, const int64_t* ngm_W,
+               const int* nm_W, const int* M_W, int nB, const int* G_B,
+               const int* W_B, double dv, int nq, const double* phase_qW,
+               int64_t nG, int nM, gb_lfc** out);
+int gb_lfc_add(const gb_lfc* lfc, const void* c_xM, void* a_xG, int64_t nx,
+               int dtype, int q, void* stream);
+int gb_lfc_integrate(const gb_lfc* lfc, const void* a_xG, void* c_xM,
+                     int64_t nx, int dtype, int q, void* stream);
+int gb_lfc_free(gb_lfc* lfc);
+
+/* ======================================================================
  * Exchange-correlation on the grid  -- replaces _gpaw.XCFunctional.calculate
  *   reference: c/xc/xc.c:73-227 (spin-paired / polarised drivers),
  *              c/xc/pbe.c (PBE exchange + PW92/PBE correlation),

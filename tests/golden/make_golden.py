@@ -213,3 +213,83 @@ def main():
 
 if __name__ == '__main__':
     main()
+
+
+# ---------------------------------------------------------------- LFC
+from lfc_cases import LFC_CASES  # noqa: E402
+
+
+def lfc_golden():
+    """Reference-built LFC data: _gpaw.spline_to_grid for every box of
+    gd.get_boxes (restated from gpaw/grid_descriptor.py:344-411 in
+    gpaw_b200.grid_descriptor), the boundary sort of gpaw/lfc.py:330-344 and
+    _gpaw.LFC add / integrate / derivative on seeded coefficients."""
+    sys.path.insert(0, str(REPO))
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    res = {}
+    for name, (N_c, cell, pbc, spos_ac, spl, k_c) in LFC_CASES.items():
+        gd = GridDescriptor(N_c, cell, pbc, device='cpu')
+        rs = [[_gpaw.Spline(l, rmax, np.append(np.array(f, float)[:-1], 0.0))   # Spline.from_data
+               for (l, rmax, f) in sj] for sj in spl]
+        A_W, M_W, G_l, W_l, sdisp_W, pos_W, spl_M = [], [], [], [], [], [], []
+        W = 0
+        Ma = 0
+        for a, sj in enumerate(rs):
+            M = 0
+            for s in sj:
+                l = s.get_angular_momentum_number()
+                for beg, end, sdisp in gd.get_boxes(np.array(spos_ac[a]), s.get_cutoff(), True):
+                    pos_v = np.dot(np.array(spos_ac[a]) - sdisp, gd.cell_cv)
+                    A_gm, G_b = _gpaw.spline_to_grid(s, beg, end, pos_v,
+                                                     np.ascontiguousarray(gd.h_cv), gd.n_c, gd.beg_c)
+                    if len(G_b) == 0:
+                        continue
+                    A_W.append(A_gm)
+                    M_W.append(Ma + M)
+                    G_l.append(G_b)
+                    w = np.empty(len(G_b), np.intc)
+                    w[0::2] = W
+                    w[1::2] = -W - 1
+                    W_l.append(w)
+                    sdisp_W.append(sdisp)
+                    pos_W.append(pos_v)
+                    W += 1
+                M += 2 * l + 1
+                spl_M.extend([s] * (2 * l + 1))
+            Ma += M
+        Mmax = Ma
+        G_B = np.concatenate(G_l)
+        W_B = np.concatenate(W_l)
+        idx = np.argsort(G_B, kind='mergesort')
+        G_B = np.ascontiguousarray(G_B[idx], np.intc)
+        W_B = np.ascontiguousarray(W_B[idx], np.intc)
+        M_W = np.array(M_W, np.intc)
+        cplx = k_c is not None
+        if cplx:
+            phase_qW = np.exp(2j * np.pi * np.inner(np.array([k_c]), np.array(sdisp_W)))
+        else:
+            phase_qW = np.empty((0, W), complex)
+        lfc = _gpaw.LFC(A_W, M_W, G_B, W_B, gd.dv, phase_qW)
+        rng = np.random.default_rng(7)
+        nx = 2
+        c_xM = rng.standard_normal((nx, Mmax))
+        a_xG = rng.standard_normal((nx,) + tuple(gd.n_c))
+        if cplx:
+            c_xM = c_xM + 1j * rng.standard_normal(c_xM.shape)
+            a_xG = a_xG + 1j * rng.standard_normal(a_xG.shape)
+        q = 0 if cplx else -1
+        b_xG = np.zeros_like(a_xG)
+        lfc.add(c_xM, b_xG, q)
+        i_xM = np.zeros_like(c_xM)
+        lfc.integrate(a_xG, i_xM, q)
+        d_xMv = np.zeros(c_xM.shape + (3,), c_xM.dtype)
+        lfc.derivative(a_xG, d_xMv, np.ascontiguousarray(gd.h_cv), gd.n_c, spl_M, gd.beg_c,
+                       np.array(pos_W), q)
+        res[f'{name}|add'] = b_xG
+        res[f'{name}|integrate'] = i_xM
+        res[f'{name}|derivative'] = d_xMv
+    return res
+
+
+if __name__ == '__main__':
+    np.savez_compressed(HERE / 'lfc.npz', **lfc_golden())
