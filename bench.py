@@ -272,6 +272,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-suite', action='store_true')
+    ap.add_argument('--stencil-path', type=int, default=0,
+                    help='0 auto (TMA where possible), 1 cp.async kernel, 2 TMA only')
     args = ap.parse_args()
     if args.impl == 'reference':
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count() or 1))
@@ -289,6 +291,8 @@ def main():
         dist.init_process_group('nccl', timeout=timedelta(seconds=120),
                                 device_id=torch.device('cuda', local))
     from gpaw_b200.fd_operators import Laplace
+    from gpaw_b200 import _native as nat
+    nat.check(nat.lib().gb_set_stencil_path(args.stencil_path), 'stencil path')
     stream = torch.cuda.current_stream()
     gd = grid(True)
     lap = Laplace(gd, -0.5, 3)

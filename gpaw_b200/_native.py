@@ -40,6 +40,8 @@ _SIGNATURES = {
                                   c_double, c_void_p]),
     'gb_operator_get_diagonal_element': (c_int, [c_void_p, PD]),
     'gb_operator_free': (c_int, [c_void_p]),
+    'gb_set_stencil_path': (c_int, [c_int]),
+    'gb_device_errors': (c_int, [c_int, POINTER(c_int)]),
     'gb_transformer_new': (c_int, [P64, P64, c_int, P64, P64, P64, P64, c_int,
                                    c_int, POINTER(c_void_p)]),
     'gb_transformer_apply': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,

@@ -67,20 +67,6 @@ struct StarCfg {
   static_assert((W * sizeof(T)) % 16 == 0, "row pitch must keep 16-byte alignment");
 };
 
-// 16-byte vector load of N contiguous elements from shared memory
-template <typename T, int N>
-__device__ __forceinline__ void lds_vec(const T* p, T (&v)[N]) {
-  constexpr int VEC = 16 / sizeof(T);
-  static_assert(N % VEC == 0, "");
-#pragma unroll
-  for (int i = 0; i < N / VEC; ++i) {
-    float4 x = *reinterpret_cast<const float4*>(p + i * VEC);
-    const T* e = reinterpret_cast<const T*>(&x);
-#pragma unroll
-    for (int k = 0; k < VEC; ++k) v[i * VEC + k] = e[k];
-  }
-}
-
 // true modulo: partial tiles of small grids can reach several periods away
 // (those cells feed no valid output, but their loads must stay in bounds)
 __device__ __forceinline__ int wrap_index(int i, int n) {
@@ -583,6 +569,9 @@ static int launch_box(const gb_operator* op, const void* in, void* out, int64_t 
 int op_apply(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype,
              const double* ph, cudaStream_t st, const Epilogue& ep) {
   if (op->cfd) {
+    const int rc = star_tma_apply(op, in, out, nin, dtype, ph, st, ep);
+    if (rc != 1) return rc;
+    if (stencil_path() == 2) return fail(GB_E_UNSUPPORTED, "TMA stencil path required but not applicable");
     switch (dtype) {
       case GB_DTYPE_F64: return dispatch_star<double>(op, in, out, nin, ph, st, ep);
       case GB_DTYPE_F32: return dispatch_star<float>(op, in, out, nin, ph, st, ep);

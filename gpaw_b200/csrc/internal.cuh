@@ -46,8 +46,28 @@ struct gb_transformer {
 };
 
 namespace gb {
+// 16-byte vector load of N contiguous elements from shared memory
+template <typename T, int N>
+__device__ __forceinline__ void lds_vec(const T* p, T (&v)[N]) {
+  constexpr int VEC = 16 / sizeof(T);
+  static_assert(N % VEC == 0, "");
+#pragma unroll
+  for (int i = 0; i < N / VEC; ++i) {
+    float4 x = *reinterpret_cast<const float4*>(p + i * VEC);
+    const T* e = reinterpret_cast<const T*>(&x);
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) v[i * VEC + k] = e[k];
+  }
+}
+
+
 int op_apply(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype,
              const double* ph, cudaStream_t st, const Epilogue& ep);
 int tr_apply(const gb_transformer* t, const void* in, void* out, int64_t nin, int dtype,
              const double* ph, cudaStream_t st, double alpha, const void* y, double gamma);
+// TMA stencil path: returns 1 when the request is not eligible (caller falls back)
+int star_tma_apply(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype,
+                   const double* ph, cudaStream_t st, const Epilogue& ep);
+void set_stencil_path(int mode);
+int stencil_path();
 }  // namespace gb

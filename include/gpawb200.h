@@ -76,6 +76,13 @@ int gb_operator_apply(const gb_operator* op, const void* in, void* out,
 int gb_operator_relax(const gb_operator* op, int relax_method, double* f_g,
                       const double* s_g, int nrelax, double w, void* stream);
 int gb_operator_get_diagonal_element(const gb_operator* op, double* d);
+/* Stencil kernel selection (no reference counterpart; for tests and
+ * benchmarks): 0 = automatic (TMA pipeline where the layout allows it,
+ * cp.async kernel otherwise), 1 = cp.async kernel only, 2 = TMA required. */
+int gb_set_stencil_path(int mode);
+/* Device-side error code left by a bounded wait that gave up (0 = none);
+ * clear != 0 resets it. */
+int gb_device_errors(int clear, int* code);
 int gb_operator_free(gb_operator* op);
 
 /* ======================================================================
