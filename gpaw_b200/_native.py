@@ -36,6 +36,8 @@ _SIGNATURES = {
                                 POINTER(c_void_p)]),
     'gb_operator_apply': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int,
                                   PD, c_void_p]),
+    'gb_operator_apply_potential': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,
+                                            c_int, c_void_p, PD, c_void_p]),
     'gb_operator_relax': (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int,
                                   c_double, c_void_p]),
     'gb_operator_get_diagonal_element': (c_int, [c_void_p, PD]),
@@ -55,6 +57,8 @@ _SIGNATURES = {
     'gb_lfc_integrate': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int,
                                  c_int, c_void_p]),
     'gb_lfc_free': (c_int, [c_void_p]),
+    'gb_add_to_density': (c_int, [c_int64, c_void_p, c_void_p, c_int, c_int64,
+                                  c_void_p, c_void_p]),
     'gb_xc_calculate': (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_void_p, c_void_p]),
     'gb_fd_precond': (c_int, [c_void_p] * 7 + [c_void_p] * 8 +

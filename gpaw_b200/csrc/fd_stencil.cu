@@ -45,6 +45,7 @@ struct StarArgs {
   // epilogue: out = alpha * S(in) + beta * in + gamma * y   (y may be null)
   double alpha, beta, gamma;
   const void* y;
+  const void* vpot;
 };
 
 template <typename T_, int H_, int R1_, int R2_, int TY_, int TZ_, int D_>
@@ -95,7 +96,8 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
   int64_t s = total * blockIdx.x / gridDim.x;
   const int64_t s_end = total * (blockIdx.x + 1) / gridDim.x;
 
-  const bool epi = args.alpha != 1.0 || args.beta != 0.0 || args.y != nullptr;
+  const bool epi = args.alpha != 1.0 || args.beta != 0.0 || args.y != nullptr || args.vpot != nullptr;
+  const R* __restrict__ vpot = reinterpret_cast<const R*>(args.vpot);
   const R ealpha = (R)args.alpha, ebeta = (R)args.beta, egamma = (R)args.gamma;
   R c0 = (R)args.c0;
   R a0[2 * H + 1], a1[2 * H + 1], a2[2 * H + 1];
@@ -310,6 +312,7 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
               const int z = z0 + tz * R2 + c;
               T v = fmadd(scale(ealpha, acc[r][c]), ebeta, q[H][r][c]);
               if (yp && y < n1 && z < n2) v = fmadd(v, egamma, yp[(int64_t)y * n2 + z]);
+              if (vpot && y < n1 && z < n2) v = fmadd(v, vpot[(int64_t)cpl * n12 + (int64_t)y * n2 + z], q[H][r][c]);
               acc[r][c] = v;
             }
           }
@@ -365,6 +368,7 @@ struct BoxArgs {
   double ph[3][2][2];
   double alpha, beta, gamma;
   const void* y;
+  const void* vpot;
 };
 
 template <typename T>
@@ -422,9 +426,11 @@ __global__ void __launch_bounds__(256) box_kernel(const BoxArgs args) {
         x = fmadd(x, (R)args.coef[p], tile[j]);
       }
       const int64_t gidx = (int64_t)gx * n12 + (int64_t)gy * args.n2 + gz;
-      if (args.alpha != 1.0 || args.beta != 0.0 || args.y) {
-        x = fmadd(scale((R)args.alpha, x), (R)args.beta, tile[((i0 + M) * E1 + (i1 + M)) * E2 + (i2 + M)]);
+      if (args.alpha != 1.0 || args.beta != 0.0 || args.y || args.vpot) {
+        const T xc = tile[((i0 + M) * E1 + (i1 + M)) * E2 + (i2 + M)];
+        x = fmadd(scale((R)args.alpha, x), (R)args.beta, xc);
         if (args.y) x = fmadd(x, (R)args.gamma, reinterpret_cast<const T*>(args.y)[band * n012 + gidx]);
+        if (args.vpot) x = fmadd(x, reinterpret_cast<const R*>(args.vpot)[gidx], xc);
       }
       dst[gidx] = x;
     }
@@ -484,7 +490,7 @@ static int launch_star(const gb_operator* op, const void* in, void* out, int64_t
   a.tiles2 = ceil_div(a.n2, C::T2);
   a.c0 = op->center;
   memcpy(a.a, op->a, sizeof(a.a));
-  a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma; a.y = ep.y;
+  a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma; a.y = ep.y; a.vpot = ep.vpot;
   a.has_phase = 0;
   for (int c = 0; c < 3; ++c)
     for (int d = 0; d < 2; ++d) {
@@ -670,6 +676,20 @@ int gb_operator_apply(const gb_operator* op, const void* in, void* out, int64_t 
   cudaStream_t st = (cudaStream_t)stream;
   const double* ph = dtype_complex(dtype) ? phase_cd : nullptr;
   return op_apply(op, in, out, nin, dtype, ph, st, Epilogue());
+}
+
+int gb_operator_apply_potential(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype,
+                                const void* vt, const double* phase_cd, void* stream) {
+  GB_REQUIRE(op && vt, "gb_operator_apply_potential: null operator or potential");
+  GB_REQUIRE(dtype_valid(dtype) && nin >= 0, "gb_operator_apply_potential: bad dtype or batch");
+  GB_REQUIRE(dtype_complex(dtype) == !op->real,
+             "gb_operator_apply_potential: dtype does not match the operator's real/complex flag");
+  if (nin == 0) return GB_OK;
+  GB_REQUIRE(in && out && in != out, "gb_operator_apply_potential: bad data pointers");
+  GB_REQUIRE(!dtype_complex(dtype) || phase_cd, "gb_operator_apply_potential: complex data needs phase_cd");
+  Epilogue ep;
+  ep.vpot = vt;
+  return op_apply(op, in, out, nin, dtype, dtype_complex(dtype) ? phase_cd : nullptr, (cudaStream_t)stream, ep);
 }
 
 int gb_operator_relax(const gb_operator* op, int relax_method, double* f_g, const double* s_g,

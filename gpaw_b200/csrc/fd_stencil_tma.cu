@@ -63,6 +63,7 @@ struct TmaArgs {
   double c0;
   double a[3][2 * HMAX + 1];
   double alpha, beta, gamma;
+  const void* vpot;
 };
 
 template <typename T, int H, int R1, int R2, int NS>
@@ -165,7 +166,8 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
     a1[m] = (R)a.a[1][m - H + HMAX];
     a2[m] = (R)a.a[2][m - H + HMAX];
   }
-  const bool epi = a.alpha != 1.0 || a.beta != 0.0 || a.y != nullptr;
+  const bool epi = a.alpha != 1.0 || a.beta != 0.0 || a.y != nullptr || a.vpot != nullptr;
+  const R* __restrict__ vpot = reinterpret_cast<const R*>(a.vpot);
   const R ealpha = (R)a.alpha, ebeta = (R)a.beta, egamma = (R)a.gamma;
 
   long long k = 0;
@@ -304,6 +306,7 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
             for (int c = 0; c < R2; ++c) {
               T v = fmadd(scale(ealpha, acc[r][c]), ebeta, q[H][r][c]);
               if (yp) v = fmadd(v, egamma, yp[(int64_t)yy * n2 + tz * R2 + c]);
+              if (vpot) v = fmadd(v, vpot[(int64_t)cpl * n12 + (int64_t)yy * n2 + tz * R2 + c], q[H][r][c]);
               acc[r][c] = v;
             }
           }
@@ -338,15 +341,37 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
   constexpr int NS = H + 3;
   const int n0 = (int)op->n[0], n1 = (int)op->n[1], n2 = (int)op->n[2];
   const int TZ = n2 / R2;
-  // rows per tile: periodic axis 1 needs T1 | n1 and at least two tiles
-  int best_ty = -1, best_cost = 1 << 30;
-  for (int ty = 1; ty * TZ <= 512; ++ty) {
+  auto kern = star_tma_kernel<T, H, R1, R2, NS>;
+  static int regs = -1;
+  if (regs < 0) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) return 1;
+    regs = fa.numRegs;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+  }
+  // rows per tile: periodic axis 1 needs T1 | n1 and at least two tiles;
+  // pick the tile that keeps the most consumer threads resident per SM
+  // (registers and shared memory both limit the CTAs per SM).
+  int best_ty = -1;
+  double best_score = -1.0;
+  const int64_t rowb0 = (int64_t)n2 * sizeof(T);
+  for (int ty = 1; ty * TZ <= 1024 - 32; ++ty) {
     const int T1 = ty * R1;
-    if (T1 < H) continue;
+    if (T1 < H || T1 + 2 * H > 256) continue;
     if (op->pbc[1] && (n1 % T1 != 0 || n1 / T1 < 2)) continue;
-    if (!op->pbc[1] && T1 > n1 + R1) continue;
-    const int cost = std::abs(ty * TZ - 256);
-    if (cost < best_cost) { best_cost = cost; best_ty = ty; }
+    if (!op->pbc[1] && T1 > n1 + R1 - 1) continue;
+    const int threads = ((ty * TZ + 31) / 32) * 32 + 32;
+    const int regs_cta = threads * ((regs + 7) / 8 * 8);
+    const int by_regs = 65536 / regs_cta;
+    const int64_t slot = ((T1 + 2 * H) * rowb0 + 128 + 127) / 128 * 128;
+    const int64_t smem_cta = 256 + NS * slot;
+    if (smem_cta > 220 * 1024) continue;
+    const int by_smem = (int)((228 * 1024) / (smem_cta + 1024));
+    const int ctas = std::min(by_regs, by_smem);
+    if (ctas < 1) continue;
+    // resident consumer threads, discounted by the halo re-read overhead
+    const double score = (double)ctas * ty * TZ * T1 / (T1 + 2.0 * H);
+    if (score > best_score) { best_score = score; best_ty = ty; }
   }
   if (best_ty < 0) return 1;   // not eligible
   TmaArgs a{};
@@ -359,7 +384,7 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
   a.slot_bytes = (int)(((a.ROWS * rowb + 128) + 127) / 128 * 128);
   a.c0 = op->center;
   memcpy(a.a, op->a, sizeof(a.a));
-  a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma;
+  a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma; a.vpot = ep.vpot;
   const size_t smem = 256 + (size_t)NS * a.slot_bytes;
   if (smem > 220 * 1024 || a.ROWS > 256) return 1;
   // tensor maps over (n2 scalars, n1, n0, nbatch)
@@ -378,12 +403,6 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
       !encode_tensor_map_4d(&tmH, dt, base, dims, strides, boxH) ||
       !encode_tensor_map_4d(&tmB, dt, base, dims, strides, boxB))
     return 1;
-  auto kern = star_tma_kernel<T, H, R1, R2, NS>;
-  static size_t smem_set = 0;
-  if (smem_set < smem) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    smem_set = 220 * 1024;
-  }
   const int threads = ((a.NTC + 31) / 32) * 32 + 32;
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
@@ -415,30 +434,30 @@ int star_tma_apply(const gb_operator* op, const void* in, void* out, int64_t nin
   switch (dtype) {
     case GB_DTYPE_F64:
       switch (op->H) {
-        case 1: return launch_tma_cfg<double, 1, 4, 2>(op, in, out, nin, st, ep);
-        case 2: return launch_tma_cfg<double, 2, 4, 2>(op, in, out, nin, st, ep);
-        case 3: return launch_tma_cfg<double, 3, 4, 2>(op, in, out, nin, st, ep);
+        case 1: return launch_tma_cfg<double, 1, 2, 2>(op, in, out, nin, st, ep);
+        case 2: return launch_tma_cfg<double, 2, 2, 2>(op, in, out, nin, st, ep);
+        case 3: return launch_tma_cfg<double, 3, 2, 2>(op, in, out, nin, st, ep);
         default: return launch_tma_cfg<double, 4, 2, 2>(op, in, out, nin, st, ep);
       }
     case GB_DTYPE_F32:
       switch (op->H) {
-        case 1: return launch_tma_cfg<float, 1, 4, 4>(op, in, out, nin, st, ep);
-        case 2: return launch_tma_cfg<float, 2, 4, 4>(op, in, out, nin, st, ep);
-        case 3: return launch_tma_cfg<float, 3, 4, 4>(op, in, out, nin, st, ep);
+        case 1: return launch_tma_cfg<float, 1, 2, 4>(op, in, out, nin, st, ep);
+        case 2: return launch_tma_cfg<float, 2, 2, 4>(op, in, out, nin, st, ep);
+        case 3: return launch_tma_cfg<float, 3, 2, 4>(op, in, out, nin, st, ep);
         default: return launch_tma_cfg<float, 4, 2, 4>(op, in, out, nin, st, ep);
       }
     case GB_DTYPE_C128:
       switch (op->H) {
-        case 1: return launch_tma_cfg<double2, 1, 4, 1>(op, in, out, nin, st, ep);
-        case 2: return launch_tma_cfg<double2, 2, 4, 1>(op, in, out, nin, st, ep);
-        case 3: return launch_tma_cfg<double2, 3, 4, 1>(op, in, out, nin, st, ep);
+        case 1: return launch_tma_cfg<double2, 1, 2, 1>(op, in, out, nin, st, ep);
+        case 2: return launch_tma_cfg<double2, 2, 2, 1>(op, in, out, nin, st, ep);
+        case 3: return launch_tma_cfg<double2, 3, 2, 1>(op, in, out, nin, st, ep);
         default: return launch_tma_cfg<double2, 4, 2, 1>(op, in, out, nin, st, ep);
       }
     default:
       switch (op->H) {
-        case 1: return launch_tma_cfg<float2, 1, 4, 2>(op, in, out, nin, st, ep);
-        case 2: return launch_tma_cfg<float2, 2, 4, 2>(op, in, out, nin, st, ep);
-        case 3: return launch_tma_cfg<float2, 3, 4, 2>(op, in, out, nin, st, ep);
+        case 1: return launch_tma_cfg<float2, 1, 2, 2>(op, in, out, nin, st, ep);
+        case 2: return launch_tma_cfg<float2, 2, 2, 2>(op, in, out, nin, st, ep);
+        case 3: return launch_tma_cfg<float2, 3, 2, 2>(op, in, out, nin, st, ep);
         default: return launch_tma_cfg<float2, 4, 2, 2>(op, in, out, nin, st, ep);
       }
   }

@@ -6,10 +6,13 @@
 namespace gb {
 static constexpr int HMAX = 6;   // largest axis radius handled by star_kernel
 
-// out = alpha * Op(in) + beta * in + gamma * y   (y may be null)
+// out = alpha * Op(in) + beta * in + gamma * y + vpot * in
+// (y may be null; vpot is an optional real grid of the operator's shape,
+// broadcast over bands, in the element precision: the local potential)
 struct Epilogue {
   double alpha = 1.0, beta = 0.0, gamma = 0.0;
   const void* y = nullptr;
+  const void* vpot = nullptr;
 };
 
 }  // namespace gb

@@ -1,0 +1,106 @@
+"""RMM-DIIS (drop-in for gpaw.eigensolvers.rmmdiis.RMMDIIS).
+
+The reference's algorithm (gpaw/eigensolvers/rmmdiis.py:63-272): subspace
+diagonalisation, residuals, then per band: precondition, line step
+lambda = -<R|dR>/<dR|dR>, niter-1 DIIS steps over the stored (psi, R) pairs,
+a final preconditioned trial step.  Every band's update uses only its own
+vectors, so on the GPU all bands form one block: each stencil,
+preconditioner and LFC launch covers every band, the per-band dot products
+are batched reductions and the small DIIS systems are one batched solve.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from gpaw_b200.eigensolvers.eigensolver import Eigensolver
+
+
+class RMMDIIS(Eigensolver):
+    def __init__(self, keep_htpsit=True, blocksize=None, niter=3, rtol=1e-16,
+                 limit_lambda=False, use_rayleigh=False, trial_step=0.1):
+        Eigensolver.__init__(self, keep_htpsit, blocksize)
+        self.niter = niter
+        self.rtol = rtol
+        self.limit_lambda = limit_lambda
+        self.trial_step = trial_step
+
+    def todict(self):
+        return {'name': 'rmm-diis', 'niter': self.niter}
+
+    def iterate_one_k_point(self, ham, wfs, kpt, weights):
+        self.subspace_diagonalize(ham, wfs, kpt)
+        psit = kpt.psit_nG
+        R = self.Htpsit_nG
+        q = kpt.q if wfs.dtype.is_complex else -1
+        self.calculate_residuals(kpt, wfs, ham, psit, kpt.P_ani, kpt.eps_n, R)
+        dv = wfs.gd.dv
+        nb = psit.shape[0]
+        B = nb if self.blocksize is None else self.blocksize
+        Ht = lambda x, out: wfs.apply_pseudo_hamiltonian(kpt, ham, x, out)
+
+        def dots(a, b):
+            # Re <a_n|b_n> per band
+            A = a.reshape(a.shape[0], -1)
+            Bm = b.reshape(b.shape[0], -1)
+            return (A.conj() * Bm).real.sum(dim=1, dtype=torch.float64) * dv
+
+        error = 0.0
+        for n1 in range(0, nb, B):
+            n2 = min(n1 + B, nb)
+            eps_x = kpt.eps_n[n1:n2]
+            psitb = psit[n1:n2]
+            Rb = R[n1:n2]
+            w = torch.as_tensor(weights[n1:n2], dtype=torch.float64, device=psit.device)
+            error += float((w * dots(Rb, Rb)).sum())
+            nbl = n2 - n1
+            if self.niter > 1:
+                psit_diis = torch.empty((nbl, self.niter) + psit.shape[1:],
+                                        dtype=psit.dtype, device=psit.device)
+                R_diis = torch.empty_like(psit_diis)
+                psit_diis[:, 0] = psitb
+                R_diis[:, 0] = Rb
+            dpsit = self.preconditioner(Rb, kpt)
+            dR = torch.empty_like(dpsit)
+            Ht(dpsit, dR)
+            P = wfs.projections(dpsit, kpt)
+            self.calculate_residuals(kpt, wfs, ham, dpsit, P, eps_x, dR)
+            RdR = dots(dR, Rb)
+            dRdR = dots(dR, dR)
+            lam = -RdR / dRdR
+            if self.limit_lambda:
+                lo, up = self.limit_lambda['lower'], self.limit_lambda['upper']
+                if self.limit_lambda.get('absolute', False):
+                    lam = torch.where(lam.abs() < lo, lo * lam.sign(), lam)
+                    lam = torch.where(lam.abs() > up, up * lam.sign(), lam)
+                else:
+                    lam = lam.clamp(lo, up)
+            lam_b = lam.to(wfs.real_dtype).reshape(-1, 1, 1, 1)
+            psitb += lam_b * dpsit
+            Rb += lam_b * dR
+            for nit in range(1, self.niter):
+                psit_diis[:, nit] = psitb
+                R_diis[:, nit] = Rb
+                if nit > 1 or self.limit_lambda:
+                    Rd = R_diis[:, :nit + 1].reshape(nbl, nit + 1, -1)
+                    R_nn = torch.einsum('bix,bjx->bij', Rd.conj(), Rd) * dv
+                    A = -torch.ones((nbl, nit + 2, nit + 2), dtype=torch.float64,
+                                    device=psit.device)
+                    A[:, :nit + 1, :nit + 1] = R_nn.real.to(torch.float64)
+                    A[:, -1, -1] = 0.0
+                    x = torch.zeros((nbl, nit + 2), dtype=torch.float64, device=psit.device)
+                    x[:, -1] = -1.0
+                    alpha = torch.linalg.solve(A, x)[:, :-1].to(wfs.real_dtype)
+                    al = alpha.reshape(nbl, nit + 1, 1, 1, 1)
+                    psitb.copy_((al * psit_diis[:, :nit + 1]).sum(1))
+                    Rb.copy_((al * R_diis[:, :nit + 1]).sum(1))
+                if nit < self.niter - 1:
+                    dpsit = self.preconditioner(Rb, kpt)
+                    psitb += lam_b * dpsit
+                    Ht(psitb, Rb)
+                    P = wfs.projections(psitb, kpt)
+                    self.calculate_residuals(kpt, wfs, ham, psitb, P, eps_x, Rb)
+            dpsit = self.preconditioner(Rb, kpt)
+            step = self.trial_step if self.trial_step is not None else lam_b
+            psitb += step * dpsit
+        return error

@@ -135,6 +135,26 @@ class FDOperator:
             else None, nat.stream_of(in_xg)), 'gb_operator_apply')
         return out_xg
 
+    def apply_potential(self, in_xg, out_xg, vt_g, phase_cd=None):
+        """out = op(in) + vt * in (vt: one real grid, broadcast over the
+        leading dims) in one fused pass -- the local pseudo-Hamiltonian."""
+        nat.require_cuda(in_xg, out_xg, vt_g)
+        if in_xg.shape != out_xg.shape or tuple(in_xg.shape[-3:]) != self.shape:
+            raise ValueError('shape mismatch')
+        if tuple(vt_g.shape) != self.shape:
+            raise ValueError('potential must have the grid shape')
+        real_t = torch.float32 if in_xg.dtype in (torch.float32, torch.complex64) else torch.float64
+        if vt_g.dtype != real_t:
+            raise ValueError(f'potential dtype must be {real_t}')
+        if in_xg.dtype.is_complex and phase_cd is None:
+            phase_cd = np.ones((3, 2), complex)
+        nin = int(np.prod(in_xg.shape[:-3], dtype=np.int64))
+        nat.check(nat.lib().gb_operator_apply_potential(
+            self._handle, nat.ptr(in_xg), nat.ptr(out_xg), nin, nat.dtype_code(in_xg),
+            nat.ptr(vt_g), nat.phases(phase_cd) if in_xg.dtype.is_complex else None,
+            nat.stream_of(in_xg)), 'gb_operator_apply_potential')
+        return out_xg
+
     def __call__(self, in_xg, out_xg=None, phase_cd=None):
         if out_xg is None:
             out_xg = torch.empty_like(in_xg)

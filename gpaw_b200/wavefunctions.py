@@ -1,0 +1,104 @@
+"""FD wave functions on the GPU (the parts of gpaw.wavefunctions.fd /
+fdpw that the RMM-DIIS hot path uses).
+
+* ``apply_pseudo_hamiltonian``: kinetic stencil + local potential, one fused
+  launch for all bands (gpaw/wavefunctions/fd.py:82-88).
+* ``orthonormalize``: S = dv psi^H psi (+ P dS P^H), inverse Cholesky,
+  psi <- L^-1 psi (gpaw/wavefunctions/fdpw.py:394-424).  The band-space
+  products are GEMMs in the working precision (FP32 with full-precision
+  accumulation, no TF32); the Cholesky factorisation and the triangular
+  inverse run in FP64 on the device.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from gpaw_b200.fd_operators import Laplace
+from gpaw_b200.lfc import LFC
+
+REAL_OF = {torch.float64: torch.float64, torch.float32: torch.float32,
+           torch.complex128: torch.float64, torch.complex64: torch.float32}
+
+
+def gemm_precision():
+    # FP32 band-space products at full FP32 precision (no TF32 rounding)
+    torch.backends.cuda.matmul.allow_tf32 = False
+
+
+class KPoint:
+    def __init__(self, psit_nG, q=-1, phase_cd=None, weight=1.0, k_c=None):
+        self.psit_nG = psit_nG
+        self.q = q
+        self.phase_cd = phase_cd
+        self.weight = weight
+        self.k_c = np.zeros(3) if k_c is None else np.asarray(k_c, float)
+        self.eps_n = None
+        self.f_n = None
+        self.P_ani = {}
+
+
+class FDWaveFunctions:
+    def __init__(self, gd, nbands, setups, spos_ac, dtype=torch.float64,
+                 stencil=3, kd=None):
+        self.gd = gd
+        self.nbands = nbands
+        self.setups = setups
+        self.dtype = dtype
+        self.real_dtype = REAL_OF[dtype]
+        cplx = dtype.is_complex
+        self.kin = Laplace(gd, -0.5, stencil, complex if cplx else float)
+        self.pt = LFC(gd, [s.pt_j for s in setups], kd=kd,
+                      dtype=complex if cplx else float)
+        self.pt.set_positions(spos_ac)
+        self.kpt_u = []
+        self.orthonormalized = False
+        gemm_precision()
+
+    # ------------------------------------------------------------------
+    def apply_pseudo_hamiltonian(self, kpt, ham, psit_xG, Htpsit_xG):
+        vt = ham.vt_G if self.real_dtype == torch.float64 else ham.vt_G32
+        self.kin.apply_potential(psit_xG, Htpsit_xG, vt, kpt.phase_cd)
+        return Htpsit_xG
+
+    def projections(self, psit_xG, kpt):
+        """P_ani = <p^a_i|psi_n> (LFC integrate, all bands at once)."""
+        c_axi = {}
+        cM = self.pt.integrate(psit_xG, c_axi, kpt.q if self.dtype.is_complex else -1)
+        return self.split_M(cM)
+
+    def split_M(self, c_xM):
+        return {a: c_xM[..., self.pt.M_a[a]:self.pt.M_a[a] + s.ni]
+                for a, s in enumerate(self.setups) if s.ni > 0}
+
+    def join_M(self, c_axi, xshape):
+        return self.pt._gather(c_axi, xshape, self.dtype, self.gd.device)
+
+    def matrix(self, a_nG, b_nG):
+        """dv a^H b as an (n, m) matrix (one GEMM)."""
+        A = a_nG.reshape(a_nG.shape[0], -1)
+        B = b_nG.reshape(b_nG.shape[0], -1)
+        return (A.conj() @ B.T) * self.gd.dv
+
+    def orthonormalize(self, kpt):
+        psit = kpt.psit_nG
+        S = self.matrix(psit, psit).to(torch.complex128 if self.dtype.is_complex
+                                         else torch.float64)
+        S = 0.5 * (S + S.conj().T)
+        L = torch.linalg.cholesky(S)
+        Linv = torch.linalg.solve_triangular(
+            L, torch.eye(L.shape[0], dtype=L.dtype, device=L.device), upper=False)
+        # psi_n <- sum_m Linv[n, m]^* psi_m  (S = L L^H, <phi|phi> = 1)
+        C = Linv.conj().to(self.dtype)
+        nb = psit.shape[0]
+        kpt.psit_nG = (C @ psit.reshape(nb, -1)).reshape(psit.shape)
+        kpt.P_ani = self.projections(kpt.psit_nG, kpt)
+
+    def add_to_density(self, nt_G, kpt):
+        from gpaw_b200 import _native as nat
+        f = torch.as_tensor(np.asarray(kpt.f_n, float), device=self.gd.device)
+        nb = kpt.psit_nG.shape[0]
+        nat.check(nat.lib().gb_add_to_density(
+            nb, nat.ptr(f), nat.ptr(kpt.psit_nG), nat.dtype_code(kpt.psit_nG),
+            int(np.prod(self.gd.n_c)), nat.ptr(nt_G), nat.stream_of(nt_G)),
+            'gb_add_to_density')

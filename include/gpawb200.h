@@ -71,6 +71,16 @@ int gb_operator_new(const double* coef_p, const int64_t* offset_p, int np,
 int gb_operator_apply(const gb_operator* op, const void* in, void* out,
                       int64_t nin, int dtype, const double* phase_cd,
                       void* stream);
+/* out = op(in) + vt * in for nin stacked grids: the local part of the
+ * pseudo-Hamiltonian (kinetic stencil plus local potential) in one pass.
+ * vt is one real grid of the operator's shape (device memory, FP64 for
+ * f64/c128 data, FP32 for f32/c64), shared by all grids.  No single
+ * counterpart: fuses Operator.apply with the potential multiply of
+ * gpaw/wavefunctions/fd.py:82-88 / gpaw/hamiltonian.py:437-443. */
+int gb_operator_apply_potential(const gb_operator* op, const void* in,
+                                void* out, int64_t nin, int dtype,
+                                const void* vt, const double* phase_cd,
+                                void* stream);
 /* Weighted-Jacobi relaxation sweeps (relax_method 2) used by the FD Poisson
  * solver: c/operators.c:55-97, c/bmgs/relax.c:7-66.  Real FP64 only. */
 int gb_operator_relax(const gb_operator* op, int relax_method, double* f_g,
@@ -162,6 +172,16 @@ int gb_lfc_free(gb_lfc* lfc);
 int gb_xc_calculate(int code, int nspins, int64_t ng, double* e_g,
                     const double* n_sg, double* v_sg, const double* sigma_xg,
                     double* dedsigma_xg, void* stream);
+
+/* ======================================================================
+ * Density accumulation  -- replaces _gpaw.add_to_density
+ *   reference: c/utilities.c:313- (one band per call),
+ *              gpaw/wavefunctions/fd.py:95-100 (the loop over bands)
+ * nt_G[G] += sum_n f_n[n] |psit_nG[n][G]|^2 for all nb bands in one launch;
+ * f_n (nb doubles) and nt_G (FP64) are device arrays.
+ * ==================================================================== */
+int gb_add_to_density(int64_t nb, const double* f_n, const void* psit_nG,
+                      int dtype, int64_t nG, double* nt_G, void* stream);
 
 #ifdef __cplusplus
 }
