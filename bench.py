@@ -53,14 +53,16 @@ def peaks():
     return 6650.0, 'fallback'
 
 
-def profiled_traffic():
-    """dram bytes per launch of the stencil kernel from the committed ncu
-    summary (profiles/star_kernel_f64_laplace_256x96.txt), or None."""
-    p = REPO / 'profiles' / 'star_kernel_f64_laplace_256x96.txt'
+def profiled_traffic(nb):
+    """DRAM bytes per launch of the stencil kernel: the per-grid figure of
+    the committed ncu summary (profiles/star_tma_kernel_f64_laplace_96cubed.txt,
+    a capture of a smaller batch of the same 96^3 grids; traffic grows in
+    proportion to the grids per launch) times the grids per launch, or None."""
+    p = REPO / 'profiles' / 'star_tma_kernel_f64_laplace_96cubed.txt'
     if not p.exists():
         return None
-    m = re.search(r'traffic_bytes_per_launch\s*=\s*([0-9.eE+]+)', p.read_text())
-    return float(m.group(1)) if m else None
+    m = re.search(r'traffic_bytes_per_grid\s*=\s*([0-9.eE+]+)', p.read_text())
+    return round(float(m.group(1)) * nb) if m else None
 
 
 class ClockSampler:
@@ -188,6 +190,53 @@ def suite(torch, stream):
                     out[f'interpolate_k{2 * nn}_{dname}_{bc}'] = round(rbytes / t / 1e6, 1)
                 del xf, xc, yf
             del x, y
+    # LFC add / integrate: 64 atom-centred Gaussians x (l = 0, 1, 2) with
+    # cutoff 2.5 A on the 96^3 grid (h = 0.2 A), 256 bands, FP64
+    from gpaw_b200.lfc import LFC
+    from gpaw_b200.spline import Spline
+    rc = 2.5 / BOHR
+    rr = np.linspace(0, rc, 101)
+    f = np.exp(-(rr / (0.8 / BOHR))**2)
+    gdl = grid(True)
+    lfc = LFC(gdl, [[Spline.from_data(l, rc, f) for l in (0, 1, 2)]] * 64)
+    lfc.set_positions(np.random.default_rng(0).random((64, 3)))
+    a = torch.randn((NB,) + tuple(gdl.n_c), generator=g, device='cuda', dtype=torch.float64)
+    cM = torch.randn((NB, lfc.Mmax), generator=g, device='cuda', dtype=torch.float64)
+    c_axi = {i: cM[:, 9 * i:9 * i + 9].contiguous() for i in range(64)}
+    # grid points covered by at least one sphere (the union over atoms)
+    cover = np.zeros(int(np.prod(gdl.n_c)), bool)
+    for sp in lfc.sphere_a:
+        for G_b in sp.G_wb:
+            for g0, g1 in zip(G_b[0::2], G_b[1::2]):
+                cover[g0:g1] = True
+    npts = int(cover.sum())
+    lfc.add(a, c_axi)
+    t = time_launches(lambda: lfc.add(a, c_axi), 5, stream)
+    # algorithmic bytes: read + write every covered point of every band
+    out['lfc_add_f64_64atoms_256bands_ms'] = round(t, 3)
+    out['lfc_add_f64_GBps'] = round(NB * 2 * npts * 8 / t / 1e6, 1)
+    lfc.integrate(a, {})
+    t = time_launches(lambda: lfc.integrate(a, {}), 5, stream)
+    out['lfc_integrate_f64_64atoms_256bands_ms'] = round(t, 3)
+    out['lfc_integrate_f64_GBps'] = round(NB * npts * 8 / t / 1e6, 1)
+    out['lfc_covered_points'] = npts
+    del a, cM, c_axi, lfc
+    # XC on the fine grid of the H2O-cluster config (151^3), FP64
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.xc import XCKernel
+    ng = 151**3
+    n_g = torch.rand((1, ng), generator=g, device='cuda', dtype=torch.float64) + 1e-3
+    sig = torch.rand((1, ng), generator=g, device='cuda', dtype=torch.float64)
+    e_g = torch.empty(ng, dtype=torch.float64, device='cuda')
+    v_g = torch.zeros_like(n_g)
+    d_g = torch.empty_like(sig)
+    for name, arrays in (('LDA', 4), ('PBE', 6)):
+        k = XCKernel(name)
+        call = (lambda: k.calculate(e_g, n_g, v_g)) if name == 'LDA' else (
+            lambda: k.calculate(e_g, n_g, v_g, sig, d_g))
+        call()
+        t = time_launches(call, 5, stream)
+        out[f'xc_{name}_151cubed_GBps'] = round(arrays * ng * 8 / t / 1e6, 1)
     # V-cycle on 160 bands of the Si64 grid (56^3, periodic), FP64
     from gpaw_b200.grid_descriptor import GridDescriptor
     gd = GridDescriptor((56, 56, 56), (20.52, 20.52, 20.52), True)
@@ -274,6 +323,12 @@ def main():
     ap.add_argument('--no-suite', action='store_true')
     ap.add_argument('--stencil-path', type=int, default=0,
                     help='0 auto (TMA where possible), 1 cp.async kernel, 2 TMA only')
+    ap.add_argument('--bands', type=int, default=NB,
+                    help='grids per step (256 is the benchmark workload; smaller '
+                         'values give the small case that ncu captures)')
+    ap.add_argument('--kernel-only', action='store_true',
+                    help='time the stencil step only (no e2e, suite or CPU '
+                         'baseline): the command line used for ncu captures')
     args = ap.parse_args()
     if args.impl == 'reference':
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count() or 1))
@@ -297,9 +352,20 @@ def main():
     gd = grid(True)
     lap = Laplace(gd, -0.5, 3)
     g = torch.Generator(device='cuda').manual_seed(0)
-    x = torch.randn((NB, N, N, N), generator=g, device='cuda', dtype=torch.float64)
+    nb = args.bands
+    x = torch.randn((nb, N, N, N), generator=g, device='cuda', dtype=torch.float64)
     y = torch.empty_like(x)
     nbytes = 2 * x.numel() * 8
+    # which stencil kernel serves this layout: try the TMA pipeline alone
+    nat.check(nat.lib().gb_set_stencil_path(2), 'stencil path')
+    try:
+        lap.apply(x[:1], y[:1])
+        kernel = 'star_tma_kernel<double,H=3,R1=2,R2=2>'
+    except nat.GPAWB200Error:
+        kernel = 'star_kernel<double,H=3>'
+    nat.check(nat.lib().gb_set_stencil_path(args.stencil_path), 'stencil path')
+    if args.stencil_path == 1:
+        kernel = 'star_kernel<double,H=3>'
 
     for _ in range(max(args.warmup, 3)):
         lap.apply(x, y)
@@ -332,6 +398,16 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = t.item()
     value = world * nbytes * args.steps / (total_ms / 1e3) / 1e9
+
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({'metric': METRIC, 'value': round(value, 1), 'unit': 'GB/s',
+                              'bands': nb, 'kernel': kernel,
+                              'ms_per_step': round(total_ms / args.steps, 4),
+                              'launch_ms': round(launch_ms, 4), 'clocks': clk}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     # e2e through the public API with host buffers (pinned), fewer steps
     e2e_steps = min(args.steps, 3)
@@ -379,29 +455,29 @@ def main():
 
     peak, peak_kind = peaks()
     achieved = nbytes / (launch_ms / 1e3) / 1e9
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(nb)
     line = {
         'metric': METRIC, 'value': round(value, 1), 'unit': 'GB/s',
         'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': round(total_ms / args.steps, 4),
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f64', 'data': 'synthetic N(0,1), seeded (torch.Generator seed 0)',
-        'config': {'workload': 'laplace_nn3_f64_periodic_256x96^3',
-                   'grid': [NB, N, N, N], 'h_angstrom': H_ANG,
+        'config': {'workload': f'laplace_nn3_f64_periodic_{nb}x96^3',
+                   'grid': [nb, N, N, N], 'h_angstrom': H_ANG,
                    'stencil': '19-point order-6 kinetic Laplacian',
                    'l2': 'inputs 1.8 GB > L2, no flush',
                    'parallelism': f'replicas x{world}'},
         'clocks': clk,
         'e2e': {'value': round(e2e_value, 2), 'unit': 'GB/s',
-                'h2d_bytes_per_step': NB * N**3 * 8,
-                'd2h_bytes_per_step': NB * N**3 * 8,
+                'h2d_bytes_per_step': nb * N**3 * 8,
+                'd2h_bytes_per_step': nb * N**3 * 8,
                 'steps': e2e_steps},
         'gpu_launches': args.steps,
         'roofline': {'bound': 'hbm', 'achieved': round(achieved, 1),
                      'peak': peak, 'unit': 'GB/s', 'frac': round(achieved / peak, 4),
                      'peak_kind': peak_kind,
                      'traffic': traffic,
-                     'kernel': 'star_kernel<double,H=3>'},
+                     'kernel': kernel},
         'cpu_baseline': cpu,
         'suite_GBps': suite_res,
     }

@@ -59,6 +59,11 @@ _SIGNATURES = {
     'gb_lfc_free': (c_int, [c_void_p]),
     'gb_add_to_density': (c_int, [c_int64, c_void_p, c_void_p, c_int, c_int64,
                                   c_void_p, c_void_p]),
+    'gb_conv3d_forward': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int,
+                                  c_int, P64, POINTER(c_int), c_int, c_void_p]),
+    'gb_conv3d_backward_weight': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,
+                                          c_int, c_int, P64, POINTER(c_int),
+                                          c_void_p]),
     'gb_xc_calculate': (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_void_p, c_void_p]),
     'gb_fd_precond': (c_int, [c_void_p] * 7 + [c_void_p] * 8 +

@@ -40,6 +40,7 @@ struct StarArgs {
   int tiles1, tiles2;
   int has_phase;
   double c0;
+  double c0diff;              // c0 + sum of the neighbour coefficients (difference form)
   double a[3][2 * HMAX + 1];  // a[axis][m + HMAX]: coefficient of offset m (m != 0)
   double ph[3][2][2];         // ph[axis][side][re/im]
   // epilogue: out = alpha * S(in) + beta * in + gamma * y   (y may be null)
@@ -99,7 +100,10 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
   const bool epi = args.alpha != 1.0 || args.beta != 0.0 || args.y != nullptr || args.vpot != nullptr;
   const R* __restrict__ vpot = reinterpret_cast<const R*>(args.vpot);
   const R ealpha = (R)args.alpha, ebeta = (R)args.beta, egamma = (R)args.gamma;
-  R c0 = (R)args.c0;
+  // FP32: the difference form sum_p c_p (x_p - x_c) + (sum c) x_c keeps the
+  // operator exactly constant-annihilating after the coefficients are rounded
+  constexpr bool DIFF = sizeof(R) == 4;
+  R c0 = DIFF ? (R)args.c0diff : (R)args.c0;
   R a0[2 * H + 1], a1[2 * H + 1], a2[2 * H + 1];
 #pragma unroll
   for (int m = 0; m <= 2 * H; ++m) {
@@ -269,7 +273,7 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
             T x = scale(c0, q[H][r][c]);
 #pragma unroll
             for (int m = 0; m <= 2 * H; ++m)
-              if (m != H) x = fmadd(x, a0[m], q[m][r][c]);
+              if (m != H) x = fmadd(x, a0[m], DIFF ? sub(q[m][r][c], q[H][r][c]) : q[m][r][c]);
 #pragma unroll
             for (int m = 0; m <= 2 * H; ++m) {
               if (m == H) continue;
@@ -278,7 +282,7 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
               if (cc < 0) v = wl[HZ + cc];
               else if (cc >= R2) v = wr[cc - R2];
               else v = q[H][r][cc];
-              x = fmadd(x, a2[m], v);
+              x = fmadd(x, a2[m], DIFF ? sub(v, q[H][r][c]) : v);
             }
             acc[r][c] = x;
           }
@@ -298,7 +302,8 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
             const int m = rr - r + H;
             if (m < 0 || m > 2 * H || m == H) continue;
 #pragma unroll
-            for (int c = 0; c < R2; ++c) acc[r][c] = fmadd(acc[r][c], a1[m], v[c]);
+            for (int c = 0; c < R2; ++c)
+              acc[r][c] = fmadd(acc[r][c], a1[m], DIFF ? sub(v[c], q[H][r][c]) : v[c]);
           }
         }
         // epilogue (fused axpy passes of the multigrid V-cycle)
@@ -369,6 +374,7 @@ struct BoxArgs {
   double alpha, beta, gamma;
   const void* y;
   const void* vpot;
+  double csum;   // sum of all coefficients (difference form in FP32)
 };
 
 template <typename T>
@@ -420,10 +426,12 @@ __global__ void __launch_bounds__(256) box_kernel(const BoxArgs args) {
       const int i2 = e % args.b2, i1 = (e / args.b2) % args.b1, i0 = e / (args.b1 * args.b2);
       const int gx = x0 + i0, gy = y0 + i1, gz = z0 + i2;
       if (gx >= args.n0 || gy >= args.n1 || gz >= args.n2) continue;
-      T x = zero<T>();
+      constexpr bool DIFF = sizeof(R) == 4;
+      const T xc0 = tile[((i0 + M) * E1 + (i1 + M)) * E2 + (i2 + M)];
+      T x = DIFF ? scale((R)args.csum, xc0) : zero<T>();
       for (int p = 0; p < args.np; ++p) {
         const int j = ((i0 + M + args.off[p][0]) * E1 + (i1 + M + args.off[p][1])) * E2 + (i2 + M + args.off[p][2]);
-        x = fmadd(x, (R)args.coef[p], tile[j]);
+        x = fmadd(x, (R)args.coef[p], DIFF ? sub(tile[j], xc0) : tile[j]);
       }
       const int64_t gidx = (int64_t)gx * n12 + (int64_t)gy * args.n2 + gz;
       if (args.alpha != 1.0 || args.beta != 0.0 || args.y || args.vpot) {
@@ -489,6 +497,9 @@ static int launch_star(const gb_operator* op, const void* in, void* out, int64_t
   a.tiles1 = ceil_div(a.n1, C::T1);
   a.tiles2 = ceil_div(a.n2, C::T2);
   a.c0 = op->center;
+  a.c0diff = op->center;
+  for (int c = 0; c < 3; ++c)
+    for (int m = 0; m < 2 * HMAX + 1; ++m) a.c0diff += op->a[c][m];
   memcpy(a.a, op->a, sizeof(a.a));
   a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma; a.y = ep.y; a.vpot = ep.vpot;
   a.has_phase = 0;
@@ -537,8 +548,10 @@ static void fill_box_args(const gb_operator* op, BoxArgs& a, const double* phase
   a.pbc0 = op->pbc[0]; a.pbc1 = op->pbc[1]; a.pbc2 = op->pbc[2];
   a.M = op->range;
   a.np = op->np;
+  a.csum = 0.0;
   for (int p = 0; p < op->np; ++p) {
     a.coef[p] = op->coef[p];
+    a.csum += op->coef[p];
     for (int c = 0; c < 3; ++c) a.off[p][c] = op->off[p * 3 + c];
   }
   for (int c = 0; c < 3; ++c)
@@ -577,7 +590,8 @@ int op_apply(const gb_operator* op, const void* in, void* out, int64_t nin, int 
   if (op->cfd) {
     const int rc = star_tma_apply(op, in, out, nin, dtype, ph, st, ep);
     if (rc != 1) return rc;
-    if (stencil_path() == 2) return fail(GB_E_UNSUPPORTED, "TMA stencil path required but not applicable");
+    if (stencil_path() == 2)
+      return fail(GB_E_UNSUPPORTED, std::string("TMA stencil path required but not applicable: ") + tma_reason());
     switch (dtype) {
       case GB_DTYPE_F64: return dispatch_star<double>(op, in, out, nin, ph, st, ep);
       case GB_DTYPE_F32: return dispatch_star<float>(op, in, out, nin, ph, st, ep);

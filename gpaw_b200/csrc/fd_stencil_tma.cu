@@ -52,6 +52,7 @@ bool encode_tensor_map_4d(CUtensorMap* map, CUtensorMapDataType dt, void* base, 
   return r == CUDA_SUCCESS;
 }
 
+static thread_local const char* g_tma_reason = "";
 struct TmaArgs {
   void* out;
   const void* y;
@@ -61,6 +62,7 @@ struct TmaArgs {
   int TY, TZ, NTC, T1, ROWS, ytiles;
   int slot_bytes;
   double c0;
+  double c0diff;   // c0 + sum of the neighbour coefficients (difference form)
   double a[3][2 * HMAX + 1];
   double alpha, beta, gamma;
   const void* vpot;
@@ -158,7 +160,11 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
   // -------------------------------------------------------------- consumers
   const bool active = tid < a.NTC;
   const int ty = active ? tid / a.TZ : 0, tz = active ? tid % a.TZ : 0;
-  const R c0 = (R)a.c0;
+  // FP32: the difference form sum_p c_p (x_p - x_c) + (sum c) x_c keeps the
+  // operator exactly constant-annihilating after the coefficients are rounded
+  // (otherwise every eigenvalue shifts by ~|c0| 2^-24)
+  constexpr bool DIFF = sizeof(R) == 4;
+  const R c0 = DIFF ? (R)a.c0diff : (R)a.c0;
   R a0[2 * H + 1], a1[2 * H + 1], a2[2 * H + 1];
 #pragma unroll
   for (int m = 0; m <= 2 * H; ++m) {
@@ -263,7 +269,7 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
             T x = scale(c0, q[H][r][c]);
 #pragma unroll
             for (int m = 0; m <= 2 * H; ++m)
-              if (m != H) x = fmadd(x, a0[m], q[m][r][c]);
+              if (m != H) x = fmadd(x, a0[m], DIFF ? sub(q[m][r][c], q[H][r][c]) : q[m][r][c]);
 #pragma unroll
             for (int m = 0; m <= 2 * H; ++m) {
               if (m == H) continue;
@@ -272,7 +278,7 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
               if (cc < 0) v = wl[HZ + cc];
               else if (cc >= R2) v = wr[cc - R2];
               else v = q[H][r][cc];
-              x = fmadd(x, a2[m], v);
+              x = fmadd(x, a2[m], DIFF ? sub(v, q[H][r][c]) : v);
             }
             acc[r][c] = x;
           }
@@ -291,7 +297,8 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
             const int m = rr - r + H;
             if (m < 0 || m > 2 * H || m == H) continue;
 #pragma unroll
-            for (int c = 0; c < R2; ++c) acc[r][c] = fmadd(acc[r][c], a1[m], v[c]);
+            for (int c = 0; c < R2; ++c)
+              acc[r][c] = fmadd(acc[r][c], a1[m], DIFF ? sub(v[c], q[H][r][c]) : v[c]);
           }
         }
         T* outp = dst + (int64_t)cpl * n12;
@@ -345,17 +352,20 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
   static int regs = -1;
   if (regs < 0) {
     cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) return 1;
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) { g_tma_reason = "cudaFuncGetAttributes failed"; return 1; }
     regs = fa.numRegs;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
   }
   // rows per tile: periodic axis 1 needs T1 | n1 and at least two tiles;
   // pick the tile that keeps the most consumer threads resident per SM
   // (registers and shared memory both limit the CTAs per SM).
-  int best_ty = -1;
-  double best_score = -1.0;
+  // candidate tiles, best score first; the first one the occupancy
+  // calculator accepts is used
+  struct Cand { double score; int ty; };
+  Cand cands[64];
+  int ncand = 0;
   const int64_t rowb0 = (int64_t)n2 * sizeof(T);
-  for (int ty = 1; ty * TZ <= 1024 - 32; ++ty) {
+  for (int ty = 1; ty * TZ <= 1024 - 32 && ncand < 64; ++ty) {
     const int T1 = ty * R1;
     if (T1 < H || T1 + 2 * H > 256) continue;
     if (op->pbc[1] && (n1 % T1 != 0 || n1 / T1 < 2)) continue;
@@ -370,10 +380,27 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
     const int ctas = std::min(by_regs, by_smem);
     if (ctas < 1) continue;
     // resident consumer threads, discounted by the halo re-read overhead
-    const double score = (double)ctas * ty * TZ * T1 / (T1 + 2.0 * H);
-    if (score > best_score) { best_score = score; best_ty = ty; }
+    cands[ncand++] = {(double)ctas * ty * TZ * T1 / (T1 + 2.0 * H), ty};
   }
-  if (best_ty < 0) return 1;   // not eligible
+  std::sort(cands, cands + ncand, [](const Cand& x, const Cand& y) { return x.score > y.score; });
+  int best_ty = -1, occ = 0, threads = 0;
+  size_t smem = 0;
+  for (int c = 0; c < ncand && best_ty < 0; ++c) {
+    const int ty = cands[c].ty;
+    const int T1 = ty * R1;
+    const int slotb = (int)((((T1 + 2 * H) * rowb0 + 128) + 127) / 128 * 128);
+    const size_t sm = 256 + (size_t)NS * slotb;
+    const int th = ((ty * TZ + 31) / 32) * 32 + 32;
+    int o = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, th, sm) == cudaSuccess && o >= 1) {
+      best_ty = ty; occ = o; threads = th; smem = sm;
+    }
+  }
+  cudaGetLastError();
+  if (best_ty < 0) {
+    g_tma_reason = ncand ? "zero occupancy" : "no row tile fits the grid (periodic axis 1 needs T1 | n1)";
+    return 1;
+  }
   TmaArgs a{};
   a.out = out; a.y = ep.y; a.nbatch = nin;
   a.n0 = n0; a.n1 = n1; a.n2 = n2;
@@ -383,10 +410,12 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
   const int64_t rowb = (int64_t)n2 * sizeof(T);
   a.slot_bytes = (int)(((a.ROWS * rowb + 128) + 127) / 128 * 128);
   a.c0 = op->center;
+  a.c0diff = op->center;
+  for (int c = 0; c < 3; ++c)
+    for (int m = 0; m < 2 * HMAX + 1; ++m) a.c0diff += op->a[c][m];
   memcpy(a.a, op->a, sizeof(a.a));
   a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma; a.vpot = ep.vpot;
-  const size_t smem = 256 + (size_t)NS * a.slot_bytes;
-  if (smem > 220 * 1024 || a.ROWS > 256) return 1;
+  if (smem > 220 * 1024 || a.ROWS > 256) { g_tma_reason = "tile too large"; return 1; }
   // tensor maps over (n2 scalars, n1, n0, nbatch)
   const int scal = Elem<T>::cplx ? 2 : 1;
   const CUtensorMapDataType dt = sizeof(typename Elem<T>::R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
@@ -401,12 +430,10 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
   void* base = const_cast<void*>(in);
   if (!encode_tensor_map_4d(&tmA, dt, base, dims, strides, boxA) ||
       !encode_tensor_map_4d(&tmH, dt, base, dims, strides, boxH) ||
-      !encode_tensor_map_4d(&tmB, dt, base, dims, strides, boxB))
+      !encode_tensor_map_4d(&tmB, dt, base, dims, strides, boxB)) {
+    g_tma_reason = "cuTensorMapEncodeTiled rejected the layout";
     return 1;
-  const int threads = ((a.NTC + 31) / 32) * 32 + 32;
-  int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
-  if (occ < 1) return 1;
+  }
   const int64_t total = nin * (int64_t)a.ytiles * n0;
   int64_t blocks = (int64_t)sm_count() * occ;
   blocks = std::min<int64_t>(blocks, std::max<int64_t>(1, total / (4 * H + 4)));
@@ -416,21 +443,26 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
 }
 
 static int g_stencil_path = 0;   // 0 auto, 1 cp.async only, 2 TMA required
+const char* tma_reason() { return g_tma_reason; }
 
 int star_tma_apply(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype, const double* ph,
                    cudaStream_t st, const Epilogue& ep) {
-  if (g_stencil_path == 1) return 1;
-  if (!op->cfd || op->H > 4) return 1;
+  g_tma_reason = "";
+  if (g_stencil_path == 1) { g_tma_reason = "cp.async path forced"; return 1; }
+  if (!op->cfd || op->H > 4) { g_tma_reason = "stencil not on axes or radius > 4"; return 1; }
   if (ph) {
     for (int i = 0; i < 6; ++i)
-      if (ph[2 * i] != 1.0 || ph[2 * i + 1] != 0.0) return 1;
+      if (ph[2 * i] != 1.0 || ph[2 * i + 1] != 0.0) { g_tma_reason = "Bloch phases"; return 1; }
   }
   const size_t es = dtype_size(dtype);
   const int n2 = (int)op->n[2];
-  if ((n2 * es) % 16 != 0 || n2 * es / (dtype_complex(dtype) ? es / 2 : es) > 256) return 1;
-  if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) return 1;
-  if (ep.y && (reinterpret_cast<uintptr_t>(ep.y) & 15)) return 1;
-  if (op->n[0] < op->H || op->n[1] < op->H) return 1;
+  if ((n2 * es) % 16 != 0 || n2 * es / (dtype_complex(dtype) ? es / 2 : es) > 256) {
+    g_tma_reason = "row pitch not a multiple of 16 bytes or row longer than a TMA box";
+    return 1;
+  }
+  if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) { g_tma_reason = "unaligned data"; return 1; }
+  if (ep.y && (reinterpret_cast<uintptr_t>(ep.y) & 15)) { g_tma_reason = "unaligned y"; return 1; }
+  if (op->n[0] < op->H || op->n[1] < op->H) { g_tma_reason = "grid shorter than the stencil"; return 1; }
   switch (dtype) {
     case GB_DTYPE_F64:
       switch (op->H) {

@@ -72,5 +72,6 @@ int tr_apply(const gb_transformer* t, const void* in, void* out, int64_t nin, in
 int star_tma_apply(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype,
                    const double* ph, cudaStream_t st, const Epilogue& ep);
 void set_stencil_path(int mode);
+const char* tma_reason();
 int stencil_path();
 }  // namespace gb

@@ -60,9 +60,11 @@ class Eigensolver:
         Htpsit = torch.empty_like(psit)
         wfs.apply_pseudo_hamiltonian(kpt, ham, psit, Htpsit)
         H = wfs.matrix(psit, Htpsit)
+        wide = torch.complex128 if wfs.dtype.is_complex else torch.float64
         for a, P in kpt.P_ani.items():
-            H = H + P.conj() @ ham.dH_aii[a].to(P.dtype) @ P.T
-        H64 = H.to(torch.complex128 if wfs.dtype.is_complex else torch.float64)
+            Pw = P.to(wide)
+            H = H + Pw.conj() @ ham.dH_aii[a].to(wide) @ Pw.T
+        H64 = H
         H64 = 0.5 * (H64 + H64.conj().T)
         eps, V = torch.linalg.eigh(H64)
         # phi_k = sum_m V[m, k] psi_m

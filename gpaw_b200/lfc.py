@@ -284,6 +284,8 @@ class LocalizedFunctionsCollection(BaseLFC):
         else:
             c_xM = self._gather(c_axi, xshape, a_xG.dtype, a_xG.device)
         nx = int(np.prod(xshape, dtype=np.int64))
+        if self.Mmax == 0:
+            return
         nat.check(nat.lib().gb_lfc_add(
             self.lfc.handle, nat.ptr(c_xM), nat.ptr(a_xG), nx,
             nat.dtype_code(a_xG), self._nq(a_xG, q), nat.stream_of(a_xG)),
@@ -295,6 +297,8 @@ class LocalizedFunctionsCollection(BaseLFC):
         xshape = tuple(a_xG.shape[:-3])
         c_xM = torch.zeros(xshape + (self.Mmax,), dtype=a_xG.dtype, device=a_xG.device)
         nx = int(np.prod(xshape, dtype=np.int64))
+        if self.Mmax == 0:
+            return c_xM
         nat.check(nat.lib().gb_lfc_integrate(
             self.lfc.handle, nat.ptr(a_xG), nat.ptr(c_xM), nx,
             nat.dtype_code(a_xG), self._nq(a_xG, q), nat.stream_of(a_xG)),

@@ -55,11 +55,27 @@ class PulayMixer:
     """Pulay (DIIS) density mixing on the coarse grid (the role of
     gpaw/mixer.py:35-; plain Euclidean metric)."""
 
-    def __init__(self, beta=0.1, nmaxold=5):
+    def __init__(self, beta=0.1, nmaxold=5, kerker_q0=None):
         self.beta = beta
         self.nmaxold = nmaxold
+        self.kerker_q0 = kerker_q0
+        self.gd = None
         self.nin = []
         self.res = []
+
+    def _precondition(self, r_G):
+        """Kerker filter k^2 / (k^2 + q0^2) on the residual (periodic cells):
+        damps the long-wavelength charge sloshing of the density update."""
+        if not self.kerker_q0 or self.gd is None:
+            return r_G
+        gd = self.gd
+        ks = [2 * np.pi * np.fft.fftfreq(gd.N_c[c], gd.cell_cv[c, c] / gd.N_c[c])
+              for c in range(3)]
+        k2 = (ks[0][:, None, None]**2 + ks[1][None, :, None]**2 +
+              ks[2][None, None, :]**2)
+        f = torch.from_numpy(k2 / (k2 + self.kerker_q0**2)).to(r_G.device)
+        f[0, 0, 0] = 1.0
+        return torch.fft.ifftn(torch.fft.fftn(r_G) * f).real
 
     def reset(self):
         self.nin, self.res = [], []
@@ -86,7 +102,7 @@ class PulayMixer:
             alpha[-1] = 1.0
         new = torch.zeros_like(nin_G)
         for a, n, r in zip(alpha, self.nin, self.res):
-            new += a * (n + self.beta * r)
+            new += a * (n + self.beta * self._precondition(r))
         return new
 
 
@@ -111,7 +127,7 @@ class Calculation:
     def __init__(self, symbols, positions, cell, pbc, h=0.2, nbands=None,
                  xc='LDA', precision='fp64', k_c=None, preconditioner=None,
                  mixer_beta=None, seed=0, device='cuda', stencil=3,
-                 r_gauss=0.6):
+                 r_gauss=0.6, kerker_q0=1.0):
         cell = np.array(cell, float)
         cell_cv = np.diag(cell) if cell.ndim == 1 else cell
         self.cell_cv = cell_cv / Bohr
@@ -145,9 +161,9 @@ class Calculation:
         self.wfs = FDWaveFunctions(self.gd, self.nbands, self.setups, self.spos_ac,
                                    dtype, stencil, kd)
         # fine-grid LFCs: short-range local potential, ion charges, density guess
-        self.vbar = LFC(self.finegd, [[s.vbar] for s in self.setups])
+        self.vbar = LFC(self.finegd, [[s.vbar] for s in self.setups], cut=True)
         self.vbar.set_positions(self.spos_ac)
-        self.ghat = LFC(self.finegd, [[s.ghat] for s in self.setups],
+        self.ghat = LFC(self.finegd, [[s.ghat] for s in self.setups], cut=True,
                         integral=[float(s.Z) for s in self.setups])
         self.ghat.set_positions(self.spos_ac)
         self.vbar_g = self.finegd.zeros()
@@ -159,7 +175,10 @@ class Calculation:
         self.poisson = FastPoissonSolver(nn=3)
         self.poisson.set_grid_descriptor(self.finegd)
         self.xc = XC(xc)
-        self.mixer = PulayMixer(beta=mixer_beta or (0.1 if self.pbc.all() else 0.25))
+        periodic = bool(self.pbc.all())
+        self.mixer = PulayMixer(beta=mixer_beta or (0.25 if periodic else 0.25),
+                                kerker_q0=kerker_q0 if periodic else None)
+        self.mixer.gd = self.gd
         self.eigensolver = RMMDIIS()
         self.preconditioner = preconditioner or Preconditioner(
             self.gd, self.wfs.kin, complex if cplx else float, block=10)
@@ -182,7 +201,7 @@ class Calculation:
                  for _ in self.setups]
         cplx = self.dtype.is_complex
         kd = self.wfs.pt.kd if cplx else None
-        lfc = LFC(self.gd, basis, kd=kd, dtype=complex if cplx else float)
+        lfc = LFC(self.gd, basis, kd=kd, dtype=complex if cplx else float, cut=True)
         lfc.set_positions(self.spos_ac)
         rng = np.random.default_rng(self.seed)
         M = lfc.Mmax
@@ -209,7 +228,7 @@ class Calculation:
         self.wfs.orthonormalized = True
 
     def _init_density(self):
-        ng = LFC(self.gd, [[s.nguess] for s in self.setups],
+        ng = LFC(self.gd, [[s.nguess] for s in self.setups], cut=True,
                  integral=[float(s.Z) for s in self.setups])
         ng.set_positions(self.spos_ac)
         self.nt_G = self.gd.zeros()

@@ -48,7 +48,7 @@ class FDWaveFunctions:
         self.real_dtype = REAL_OF[dtype]
         cplx = dtype.is_complex
         self.kin = Laplace(gd, -0.5, stencil, complex if cplx else float)
-        self.pt = LFC(gd, [s.pt_j for s in setups], kd=kd,
+        self.pt = LFC(gd, [s.pt_j for s in setups], kd=kd, cut=True,
                       dtype=complex if cplx else float)
         self.pt.set_positions(spos_ac)
         self.kpt_u = []
@@ -75,9 +75,13 @@ class FDWaveFunctions:
         return self.pt._gather(c_axi, xshape, self.dtype, self.gd.device)
 
     def matrix(self, a_nG, b_nG):
-        """dv a^H b as an (n, m) matrix (one GEMM)."""
-        A = a_nG.reshape(a_nG.shape[0], -1)
-        B = b_nG.reshape(b_nG.shape[0], -1)
+        """dv a^H b as an (n, m) FP64 matrix (one GEMM).  The overlap and
+        subspace-Hamiltonian matrices feed Cholesky and eigh, which stay FP64,
+        so their sums over grid points are accumulated in FP64 even when
+        the wave functions are FP32 (the operands are widened on the fly)."""
+        wide = torch.complex128 if self.dtype.is_complex else torch.float64
+        A = a_nG.reshape(a_nG.shape[0], -1).to(wide)
+        B = b_nG.reshape(b_nG.shape[0], -1).to(wide)
         return (A.conj() @ B.T) * self.gd.dv
 
     def orthonormalize(self, kpt):

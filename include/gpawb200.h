@@ -183,6 +183,23 @@ int gb_xc_calculate(int code, int nspins, int64_t ng, double* e_g,
 int gb_add_to_density(int64_t nb, const double* f_n, const void* psit_nG,
                       int dtype, int64_t nG, double* nt_G, void* stream);
 
+/* ======================================================================
+ * 3x3x3 convolutions of the learned preconditioner (no reference
+ * counterpart: the network stands in for the multigrid V-cycle of
+ * c/fd_preconditioner.c inside RMM-DIIS).  x, y: FP32 (nb, C, n0, n1, n2);
+ * w: BF16 [cout][cin][27] (offsets o = (k/9-1, (k/3)%3-1, k%3-1)); FP32
+ * accumulation; pbc_c: 1 = periodic, 0 = zero padding per axis.
+ * forward: y (=|+=) conv(x); backward_weight: dw (FP32) += dL/dw.
+ * Channel pairs: (1,1), (1,16), (16,16), (16,1).
+ * ==================================================================== */
+int gb_conv3d_forward(const float* x, const void* w_bf16, float* y,
+                      int64_t nb, int cin, int cout, const int64_t n_c[3],
+                      const int pbc_c[3], int accumulate, void* stream);
+int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw,
+                              int64_t nb, int cin, int cout,
+                              const int64_t n_c[3], const int pbc_c[3],
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

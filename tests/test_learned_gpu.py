@@ -1,0 +1,60 @@
+"""GPU: the learned preconditioner's forward and backward kernels against
+the FP64 oracle (oracle/learned.py) with the same BF16-rounded weights
+(tolerance 1e-4 norm-wise relative: FP32 activations and accumulation),
+and training on (residual, multigrid correction) pairs lowers the loss."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import fd
+from oracle import learned as ol
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize('N,pbc', [((16, 16, 16), (1, 1, 1)), ((16, 12, 20), (0, 0, 0)),
+                                   ((24, 16, 16), (1, 0, 1))])
+def test_forward_backward_vs_oracle(N, pbc):
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.learned import ConvNet
+    gd = GridDescriptor(N, 0.35 * np.array(N), pbc)
+    net = ConvNet(gd, seed=3)
+    params64 = {k: v.to(torch.bfloat16).to(torch.float64).cpu().numpy()
+                for k, v in net.params.items()}
+    onet = ol.Net(fd.Grid(gd.N_c, gd.cell_cv, gd.pbc_c), params64)
+    rng = np.random.default_rng(5)
+    R = rng.standard_normal((3,) + tuple(gd.n_c))
+    T = rng.standard_normal(R.shape)
+    out = net.forward(torch.from_numpy(R).cuda(), keep=True)
+    oout = onet.forward(R)
+    assert rel(out.double().cpu().numpy(), oout) < 1e-4
+    loss, g = net.loss_and_grad(out, torch.from_numpy(T).cuda())
+    grads = net.backward(g)
+    oloss, og = ol.loss_and_grad(oout, T)
+    ograds = onet.backward(og)
+    assert abs(loss - oloss) < 1e-4 * abs(oloss)
+    for k in grads:
+        assert rel(grads[k].double().cpu().numpy(), ograds[k]) < 1e-3, k
+
+
+def test_training_reduces_loss():
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.fd_operators import Laplace
+    from gpaw_b200.preconditioner import Preconditioner
+    from gpaw_b200.learned import ConvNet
+    gd = GridDescriptor((24, 24, 24), (8.0, 8.0, 8.0), True)
+    kin = Laplace(gd, -0.5, 3)
+    P = Preconditioner(gd, kin, float)
+    g = torch.Generator(device='cuda').manual_seed(0)
+    # smooth-ish residuals: a few multigrid-preconditioned random fields
+    R = torch.randn((64,) + tuple(gd.n_c), generator=g, device='cuda', dtype=torch.float64)
+    M = P(R)
+    net = ConvNet(gd, seed=1)
+    e0 = net.relative_error(R[:16].contiguous(), M[:16]).mean()
+    net.train([(R.float(), M.float())], steps=200, lr=3e-3, batch=16, log_every=0)
+    e1 = net.relative_error(R[:16].contiguous(), M[:16]).mean()
+    assert e1 < 0.5 * e0, (e0, e1)
