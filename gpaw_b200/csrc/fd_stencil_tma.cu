@@ -7,10 +7,16 @@
 // end of the same shared-memory row (no wrap-around copies), and only the
 // axis-1 halo rows of the first / last tile need a second TMA box.  One
 // producer warp streams planes (tile + halo rows) into a ring of NS slots
-// with cp.async.bulk.tensor (zero boundaries come from the TMA out-of-bounds
-// fill); consumer warps keep the axis-0 register queue of the cp.async kernel
-// and hand each slot back through an mbarrier when its last reader is done.
-// All waits are bounded (tma.cuh).
+// with cp.async.bulk.tensor; zero boundaries come from the TMA out-of-bounds
+// fill on every axis (planes -H..-1 and n0.., rows outside 0..n1-1, and the
+// padding columns of each 128-byte-pitched shared-memory row), so the
+// consumers run without boundary branches.  Consumer warps keep the axis-0
+// neighbours in a register queue whose rotation is resolved at compile time
+// (the plane loop is unrolled by 2H+1), read the in-plane neighbours from the
+// slot with 16-byte loads at offsets fixed per thread, take the stencil
+// coefficients from the kernel-parameter bank, and hand each slot back
+// through an mbarrier when its last reader is done.  All waits are bounded
+// (tma.cuh).
 #include <algorithm>
 #include <cstring>
 #include <cudaTypedefs.h>
@@ -53,41 +59,60 @@ bool encode_tensor_map_4d(CUtensorMap* map, CUtensorMapDataType dt, void* base, 
 }
 
 static thread_local const char* g_tma_reason = "";
+constexpr int NS_MAX = 16;      // ring slots (mbarrier pairs live in the first 256 bytes)
+
 struct TmaArgs {
   void* out;
   const void* y;
+  const void* vpot;
   int64_t nbatch;
   int n0, n1, n2;
   int pbc0, pbc1, pbc2;
-  int TY, TZ, NTC, T1, ROWS, ytiles;
-  int slot_bytes;
+  int TY, TZ, NTC, T1, ROWS, ytiles, NS;
+  int pitch;        // bytes per shared-memory row (multiple of 128, >= n2 * sizeof(T))
+  int slot_bytes;   // ROWS * pitch
   double c0;
-  double c0diff;   // c0 + sum of the neighbour coefficients (difference form)
+  double c0diff;    // c0 + sum of the neighbour coefficients (difference form)
   double a[3][2 * HMAX + 1];
+  float c0f, c0difff;
+  float af[3][2 * HMAX + 1];
   double alpha, beta, gamma;
-  const void* vpot;
 };
 
-template <typename T, int H, int R1, int R2, int NS>
-__global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmH,
-                                const __grid_constant__ CUtensorMap tmB, const TmaArgs a) {
+// coefficients straight from the kernel-parameter bank (no registers held)
+template <typename R>
+__device__ __forceinline__ R coef(const TmaArgs& a, int c, int m) {
+  if constexpr (sizeof(R) == 8) return a.a[c][m];
+  else return a.af[c][m];
+}
+
+// Slot layout: ROWS rows of `pitch` bytes, logical row r = grid row y0 - H + r
+// (wrapped on a periodic axis 1).  Columns [n2, pitch) of every row are TMA
+// out-of-bounds fill (zeros); on a zero-boundary axis 2 the pitch keeps at
+// least 16 such bytes, and the halo chunks left of column 0 / right of column
+// n2 - 1 read them, so the consumers have no boundary branches at all.
+template <typename T, int H, int R1, int R2>
+__global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                        const __grid_constant__ CUtensorMap tmH,
+                                                        const __grid_constant__ CUtensorMap tmB,
+                                                        const __grid_constant__ TmaArgs a) {
   using R = typename Elem<T>::R;
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int HZ = ((H + VEC - 1) / VEC) * VEC;
+  constexpr int NQ = 2 * H + 1;
   static_assert(R2 % VEC == 0, "");
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  // 128-byte aligned base for the TMA destinations
   unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-  uint64_t* empty = full + NS;
-  unsigned char* slots = smem + 128;
+  uint64_t* empty = full + NS_MAX;
+  unsigned char* slots = smem + 256;
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   const int NWC = (a.NTC + 31) >> 5;       // consumer warps
+  const int NS = a.NS;
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
-  const int T1 = a.T1, ROWS = a.ROWS;
-  const int64_t rowb = (int64_t)n2 * sizeof(T);
+  const int T1 = a.T1;
   const int64_t n12 = (int64_t)n1 * n2;
   const int64_t total = a.nbatch * a.ytiles * n0;
   const int64_t s_begin = total * blockIdx.x / gridDim.x;
@@ -102,20 +127,13 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
   }
   __syncthreads();
 
-  // split row of a tile's slot layout (rows < rs in part 0, the rest in part 1)
-  auto split_row = [&](int y0) -> int {
-    if (a.pbc1 && y0 == 0) return H;
-    if (a.pbc1 && y0 + T1 == n1) return T1 + H;
-    return ROWS;
-  };
-  auto part1_off = [&](int rs) -> int64_t { return ((rs * rowb + 127) / 128) * 128; };
-
   if (warp == NWC) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
       tma_prefetch_desc(&tmA);
       tma_prefetch_desc(&tmH);
       tma_prefetch_desc(&tmB);
+      const int tile_kind_first = a.pbc1 ? 1 : 0;
       long long k = 0;
       int64_t s = s_begin;
       while (s < s_end) {
@@ -125,31 +143,29 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
         s += p_end - p_start;
         const int band = (int)(col / a.ytiles);
         const int y0 = (int)(col % a.ytiles) * T1;
-        const int rs = split_row(y0);
-        for (int j = p_start - H; j < p_end + H; ++j, ++k) {
+        // 0: one box; 1: first tile of a periodic axis 1; 2: last tile of it
+        const int kind = (tile_kind_first && y0 == 0) ? 1 : (a.pbc1 && y0 + T1 == n1) ? 2 : 0;
+        const int L = p_end - p_start + 2 * H;
+        for (int t = 0; t < L; ++t, ++k) {
           const int slot = (int)(k % NS);
           if (k >= NS && !mbar_wait(&empty[slot], (uint32_t)(((k / NS) - 1) & 1))) {
             raise_device_error(101);
             return;
           }
-          int sp = j;
-          if (j < 0 || j >= n0) sp = a.pbc0 ? (j < 0 ? j + n0 : j - n0) : -1;
-          if (sp < 0) {
-            mbar_arrive(&full[slot]);
-            continue;
-          }
+          int sp = p_start - H + t;
+          // periodic axis 0 wraps; a zero-boundary axis 0 reads planes -H..-1
+          // and n0..n0+H-1 as TMA out-of-bounds fill (zeros)
+          if (a.pbc0) sp = sp < 0 ? sp + n0 : (sp >= n0 ? sp - n0 : sp);
           unsigned char* dst = slots + (int64_t)slot * a.slot_bytes;
-          if (rs == ROWS) {
-            mbar_arrive_expect_tx(&full[slot], (uint32_t)(ROWS * rowb));
+          mbar_arrive_expect_tx(&full[slot], (uint32_t)a.slot_bytes);
+          if (kind == 0) {
             tma_load_4d(dst, &tmA, &full[slot], 0, y0 - H, sp, band);
-          } else if (rs == H) {        // first tile of a periodic axis 1
-            mbar_arrive_expect_tx(&full[slot], (uint32_t)(ROWS * rowb));
+          } else if (kind == 1) {
             tma_load_4d(dst, &tmH, &full[slot], 0, n1 - H, sp, band);
-            tma_load_4d(dst + part1_off(H), &tmB, &full[slot], 0, 0, sp, band);
-          } else {                     // last tile of a periodic axis 1
-            mbar_arrive_expect_tx(&full[slot], (uint32_t)(ROWS * rowb));
+            tma_load_4d(dst + H * a.pitch, &tmB, &full[slot], 0, 0, sp, band);
+          } else {
             tma_load_4d(dst, &tmB, &full[slot], 0, y0 - H, sp, band);
-            tma_load_4d(dst + part1_off(T1 + H), &tmH, &full[slot], 0, 0, sp, band);
+            tma_load_4d(dst + (T1 + H) * a.pitch, &tmH, &full[slot], 0, 0, sp, band);
           }
         }
       }
@@ -158,24 +174,32 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
   }
 
   // -------------------------------------------------------------- consumers
+  // threads beyond NTC (last warp only) mirror thread 0's reads and skip the
+  // stores, so that every consumer lane runs the same barrier protocol
   const bool active = tid < a.NTC;
-  const int ty = active ? tid / a.TZ : 0, tz = active ? tid % a.TZ : 0;
+  const int ctid = active ? tid : 0;
+  const int ty = ctid / a.TZ, tz = ctid % a.TZ;
+  const int pitch = a.pitch;
+  const int own_row = (H + ty * R1) * pitch;
+  const int own_col = tz * R2 * (int)sizeof(T);
+  int lcol[HZ / VEC], rcol[HZ / VEC];
+#pragma unroll
+  for (int ch = 0; ch < HZ / VEC; ++ch) {
+    int zl = tz * R2 - HZ + ch * VEC;
+    if (zl < 0) zl = a.pbc2 ? zl + n2 : n2;
+    int zr = tz * R2 + R2 + ch * VEC;
+    if (zr >= n2) zr = a.pbc2 ? zr - n2 : n2;
+    lcol[ch] = own_row + zl * (int)sizeof(T);
+    rcol[ch] = own_row + zr * (int)sizeof(T);
+  }
   // FP32: the difference form sum_p c_p (x_p - x_c) + (sum c) x_c keeps the
   // operator exactly constant-annihilating after the coefficients are rounded
   // (otherwise every eigenvalue shifts by ~|c0| 2^-24)
   constexpr bool DIFF = sizeof(R) == 4;
-  const R c0 = DIFF ? (R)a.c0diff : (R)a.c0;
-  R a0[2 * H + 1], a1[2 * H + 1], a2[2 * H + 1];
-#pragma unroll
-  for (int m = 0; m <= 2 * H; ++m) {
-    a0[m] = (R)a.a[0][m - H + HMAX];
-    a1[m] = (R)a.a[1][m - H + HMAX];
-    a2[m] = (R)a.a[2][m - H + HMAX];
-  }
   const bool epi = a.alpha != 1.0 || a.beta != 0.0 || a.y != nullptr || a.vpot != nullptr;
   const R* __restrict__ vpot = reinterpret_cast<const R*>(a.vpot);
-  const R ealpha = (R)a.alpha, ebeta = (R)a.beta, egamma = (R)a.gamma;
 
+  T q[NQ][R1][R2];
   long long k = 0;
   int64_t s = s_begin;
   while (s < s_end) {
@@ -185,159 +209,134 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
     s += p_end - p_start;
     const int64_t band = col / a.ytiles;
     const int y0 = (int)(col % a.ytiles) * T1;
-    const int rs = split_row(y0);
-    const int64_t off1 = part1_off(rs);
+    const int L = p_end - p_start + 2 * H;
     T* dst = reinterpret_cast<T*>(a.out) + band * n12 * n0;
     const T* ybase = a.y ? reinterpret_cast<const T*>(a.y) + band * n12 * n0 : nullptr;
-    // address of (row, col) in a slot
-    auto cell = [&](const unsigned char* base, int row, int c) -> const T* {
-      const int64_t rb = row < rs ? row * rowb : off1 + (row - rs) * rowb;
-      return reinterpret_cast<const T*>(base + rb) + c;
-    };
+    const int yrow = y0 + ty * R1;
 
-    T q[2 * H + 1][R1][R2];
+    for (int tb = 0; tb < L; tb += NQ) {
 #pragma unroll
-    for (int m = 0; m <= 2 * H; ++m)
-#pragma unroll
-      for (int r = 0; r < R1; ++r)
-#pragma unroll
-        for (int c = 0; c < R2; ++c) q[m][r][c] = zero<T>();
-
-    const int j0 = p_start - H, j1 = p_end + H;
-    const long long k0 = k;
-    for (int j = j0; j < j1; ++j, ++k) {
-      const int slot = (int)(k % NS);
-      if (!mbar_wait(&full[slot], (uint32_t)((k / NS) & 1))) {
-        raise_device_error(102);
-        return;
-      }
-      const bool zplane = (j < 0 || j >= n0) && !a.pbc0;
-      const unsigned char* P = slots + (int64_t)slot * a.slot_bytes;
-#pragma unroll
-      for (int m = 0; m < 2 * H; ++m)
+      for (int u = 0; u < NQ; ++u) {
+        const int t = tb + u;
+        if (t < L) {
+        const long long kk = k + t;
+        const int slot = (int)(kk % NS);
+        if (!mbar_wait(&full[slot], (uint32_t)((kk / NS) & 1))) {
+          raise_device_error(102);
+          return;
+        }
+        const unsigned char* P = slots + (int64_t)slot * a.slot_bytes;
 #pragma unroll
         for (int r = 0; r < R1; ++r)
+          lds_vec<T, R2>(reinterpret_cast<const T*>(P + own_row + r * pitch + own_col), q[u][r]);
+
+        if (t >= 2 * H) {
+          const int cu = (u + NQ - H) % NQ;     // centre plane in the queue (static after unrolling)
+          const int cpl = p_start + t - 2 * H;
+          const unsigned char* Pc = slots + (int64_t)((kk - H) % NS) * a.slot_bytes;
+          T acc[R1][R2];
+          // centre + axis 0 (register queue)
 #pragma unroll
-          for (int c = 0; c < R2; ++c) q[m][r][c] = q[m + 1][r][c];
-#pragma unroll
-      for (int r = 0; r < R1; ++r) {
-        T v[R2];
-        if (!zplane && active) {
-          lds_vec<T, R2>(cell(P, H + ty * R1 + r, tz * R2), v);
-        } else {
-#pragma unroll
-          for (int c = 0; c < R2; ++c) v[c] = zero<T>();
-        }
-#pragma unroll
-        for (int c = 0; c < R2; ++c) q[2 * H][r][c] = v[c];
-      }
-      const int cpl = j - H;
-      if (cpl >= p_start && active) {
-        const unsigned char* Pc = slots + (int64_t)((k - H) % NS) * a.slot_bytes;
-        T acc[R1][R2];
-        const int zl = tz * R2 - HZ, zr = tz * R2 + R2;
-#pragma unroll
-        for (int r = 0; r < R1; ++r) {
-          const int row = H + ty * R1 + r;
-          T wl[HZ], wr[HZ];
-#pragma unroll
-          for (int cch = 0; cch < HZ / VEC; ++cch) {
-            int zc = zl + cch * VEC;
-            T tmp[VEC];
-            if (zc < 0 && !a.pbc2) {
-#pragma unroll
-              for (int v = 0; v < VEC; ++v) tmp[v] = zero<T>();
-            } else {
-              if (zc < 0) zc += n2;
-              lds_vec<T, VEC>(cell(Pc, row, zc), tmp);
-            }
-#pragma unroll
-            for (int v = 0; v < VEC; ++v) wl[cch * VEC + v] = tmp[v];
-            int zc2 = zr + cch * VEC;
-            if (zc2 >= n2 && !a.pbc2) {
-#pragma unroll
-              for (int v = 0; v < VEC; ++v) tmp[v] = zero<T>();
-            } else {
-              if (zc2 >= n2) zc2 -= n2;
-              lds_vec<T, VEC>(cell(Pc, row, zc2), tmp);
-            }
-#pragma unroll
-            for (int v = 0; v < VEC; ++v) wr[cch * VEC + v] = tmp[v];
-          }
-#pragma unroll
-          for (int c = 0; c < R2; ++c) {
-            T x = scale(c0, q[H][r][c]);
-#pragma unroll
-            for (int m = 0; m <= 2 * H; ++m)
-              if (m != H) x = fmadd(x, a0[m], DIFF ? sub(q[m][r][c], q[H][r][c]) : q[m][r][c]);
-#pragma unroll
-            for (int m = 0; m <= 2 * H; ++m) {
-              if (m == H) continue;
-              const int cc = c + m - H;
-              T v;
-              if (cc < 0) v = wl[HZ + cc];
-              else if (cc >= R2) v = wr[cc - R2];
-              else v = q[H][r][cc];
-              x = fmadd(x, a2[m], DIFF ? sub(v, q[H][r][c]) : v);
-            }
-            acc[r][c] = x;
-          }
-        }
-#pragma unroll
-        for (int rr = -H; rr < R1 + H; ++rr) {
-          T v[R2];
-          if (rr >= 0 && rr < R1) {
-#pragma unroll
-            for (int c = 0; c < R2; ++c) v[c] = q[H][rr][c];
-          } else {
-            lds_vec<T, R2>(cell(Pc, H + ty * R1 + rr, tz * R2), v);
-          }
-#pragma unroll
-          for (int r = 0; r < R1; ++r) {
-            const int m = rr - r + H;
-            if (m < 0 || m > 2 * H || m == H) continue;
-#pragma unroll
-            for (int c = 0; c < R2; ++c)
-              acc[r][c] = fmadd(acc[r][c], a1[m], DIFF ? sub(v[c], q[H][r][c]) : v[c]);
-          }
-        }
-        T* outp = dst + (int64_t)cpl * n12;
-        const T* yp = ybase ? ybase + (int64_t)cpl * n12 : nullptr;
-#pragma unroll
-        for (int r = 0; r < R1; ++r) {
-          const int yy = y0 + ty * R1 + r;
-          if (yy >= n1) continue;
-          T* o = outp + (int64_t)yy * n2 + tz * R2;
-          if (epi) {
+          for (int r = 0; r < R1; ++r)
 #pragma unroll
             for (int c = 0; c < R2; ++c) {
-              T v = fmadd(scale(ealpha, acc[r][c]), ebeta, q[H][r][c]);
-              if (yp) v = fmadd(v, egamma, yp[(int64_t)yy * n2 + tz * R2 + c]);
-              if (vpot) v = fmadd(v, vpot[(int64_t)cpl * n12 + (int64_t)yy * n2 + tz * R2 + c], q[H][r][c]);
-              acc[r][c] = v;
+              const T xc = q[cu][r][c];
+              T x = scale(DIFF ? (R)a.c0difff : (R)a.c0, xc);
+#pragma unroll
+              for (int m = 0; m < NQ; ++m) {
+                if (m == H) continue;
+                const T v = q[(u + 1 + m) % NQ][r][c];
+                x = fmadd(x, coef<R>(a, 0, m + HMAX - H), DIFF ? sub(v, xc) : v);
+              }
+              acc[r][c] = x;
+            }
+          // axis 2 (halo chunks of the own rows)
+#pragma unroll
+          for (int r = 0; r < R1; ++r) {
+            T wl[HZ], wr[HZ];
+#pragma unroll
+            for (int ch = 0; ch < HZ / VEC; ++ch) {
+              T tl[VEC], tr[VEC];
+              lds_vec<T, VEC>(reinterpret_cast<const T*>(Pc + lcol[ch] + r * pitch), tl);
+              lds_vec<T, VEC>(reinterpret_cast<const T*>(Pc + rcol[ch] + r * pitch), tr);
+#pragma unroll
+              for (int v = 0; v < VEC; ++v) {
+                wl[ch * VEC + v] = tl[v];
+                wr[ch * VEC + v] = tr[v];
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < R2; ++c) {
+              const T xc = q[cu][r][c];
+#pragma unroll
+              for (int m = 0; m < NQ; ++m) {
+                if (m == H) continue;
+                const int cc = c + m - H;
+                const T v = cc < 0 ? wl[HZ + cc] : (cc >= R2 ? wr[cc - R2] : q[cu][r][cc]);
+                acc[r][c] = fmadd(acc[r][c], coef<R>(a, 2, m + HMAX - H), DIFF ? sub(v, xc) : v);
+              }
             }
           }
+          // axis 1 (rows of the centre slot)
 #pragma unroll
-          for (int c = 0; c < R2; c += VEC) {
-            float4 w4;
-            T* e = reinterpret_cast<T*>(&w4);
+          for (int rr = -H; rr < R1 + H; ++rr) {
+            T v[R2];
+            if (rr >= 0 && rr < R1) {
 #pragma unroll
-            for (int v = 0; v < VEC; ++v) e[v] = acc[r][c + v];
-            __stcs(reinterpret_cast<float4*>(o + c), w4);
+              for (int c = 0; c < R2; ++c) v[c] = q[cu][rr][c];
+            } else {
+              lds_vec<T, R2>(reinterpret_cast<const T*>(Pc + own_row + rr * pitch + own_col), v);
+            }
+#pragma unroll
+            for (int r = 0; r < R1; ++r) {
+              const int m = rr - r + H;
+              if (m < 0 || m > 2 * H || m == H) continue;
+#pragma unroll
+              for (int c = 0; c < R2; ++c)
+                acc[r][c] = fmadd(acc[r][c], coef<R>(a, 1, m + HMAX - H), DIFF ? sub(v[c], q[cu][r][c]) : v[c]);
+            }
+          }
+          // epilogue + streaming stores
+          if (active) {
+            const int64_t pbase = (int64_t)cpl * n12 + (int64_t)yrow * n2 + tz * R2;
+#pragma unroll
+            for (int r = 0; r < R1; ++r) {
+              if (yrow + r >= n1) continue;
+              const int64_t p = pbase + (int64_t)r * n2;
+              if (epi) {
+#pragma unroll
+                for (int c = 0; c < R2; ++c) {
+                  T v = fmadd(scale((R)a.alpha, acc[r][c]), (R)a.beta, q[cu][r][c]);
+                  if (ybase) v = fmadd(v, (R)a.gamma, ybase[p + c]);
+                  if (vpot) v = fmadd(v, vpot[p + c], q[cu][r][c]);
+                  acc[r][c] = v;
+                }
+              }
+#pragma unroll
+              for (int c = 0; c < R2; c += VEC) {
+                float4 w4;
+                T* e = reinterpret_cast<T*>(&w4);
+#pragma unroll
+                for (int v = 0; v < VEC; ++v) e[v] = acc[r][c + v];
+                __stcs(reinterpret_cast<float4*>(dst + p + c), w4);
+              }
+            }
           }
         }
-      }
-      // hand back the slot of plane j - H (its last reader was this step)
-      if (j - H >= j0) {
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[(int)((k - H) % NS)]);
+        // hand back the slot read as centre plane (its last reader was this step)
+        if (t >= H) {
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&empty[(int)((kk - H) % NS)]);
+        }
+        }
       }
     }
-    // segment end: release the slots of the last H planes
-    for (long long kk = (k - H > k0 ? k - H : k0); kk < k; ++kk) {
+    // segment end: release the slots of the last H planes (axis-0 neighbours only)
+    for (int t = L - H; t < L; ++t) {
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[(int)(kk % NS)]);
+      if (lane == 0) mbar_arrive(&empty[(int)((k + t) % NS)]);
     }
+    k += L;
   }
 }
 
@@ -345,27 +344,29 @@ __global__ void star_tma_kernel(const __grid_constant__ CUtensorMap tmA, const _
 template <typename T, int H, int R1, int R2>
 static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int64_t nin, cudaStream_t st,
                           const Epilogue& ep) {
-  constexpr int NS = H + 3;
+  using R = typename Elem<T>::R;
   const int n0 = (int)op->n[0], n1 = (int)op->n[1], n2 = (int)op->n[2];
   const int TZ = n2 / R2;
-  auto kern = star_tma_kernel<T, H, R1, R2, NS>;
+  auto kern = star_tma_kernel<T, H, R1, R2>;
   static int regs = -1;
   if (regs < 0) {
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) { g_tma_reason = "cudaFuncGetAttributes failed"; return 1; }
     regs = fa.numRegs;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   }
-  // rows per tile: periodic axis 1 needs T1 | n1 and at least two tiles;
-  // pick the tile that keeps the most consumer threads resident per SM
-  // (registers and shared memory both limit the CTAs per SM).
-  // candidate tiles, best score first; the first one the occupancy
-  // calculator accepts is used
-  struct Cand { double score; int ty; };
-  Cand cands[64];
+  // shared-memory row pitch: 128-byte multiple; a zero-boundary axis 2 keeps
+  // at least 16 bytes of out-of-bounds fill (zeros) after the last column
+  const int rowb = n2 * (int)sizeof(T);
+  const int pitch = ((rowb + (op->pbc[2] ? 0 : 16) + 127) / 128) * 128;
+  if (pitch / (int)sizeof(R) > 256) { g_tma_reason = "row longer than a TMA box"; return 1; }
+  // candidate (rows per tile, CTAs per SM, ring depth): score = resident
+  // consumer warps (up to 24) x halo efficiency x prefetch depth (up to 4 planes)
+  struct Cand { double score; int ty, ctas, ns; };
+  Cand cands[256];
   int ncand = 0;
-  const int64_t rowb0 = (int64_t)n2 * sizeof(T);
-  for (int ty = 1; ty * TZ <= 1024 - 32 && ncand < 64; ++ty) {
+  const int SMEM_SM = 228 * 1024, SMEM_CTA = 227 * 1024;
+  for (int ty = 1; ty * TZ <= 512 - 32 && ncand < 250; ++ty) {
     const int T1 = ty * R1;
     if (T1 < H || T1 + 2 * H > 256) continue;
     if (op->pbc[1] && (n1 % T1 != 0 || n1 / T1 < 2)) continue;
@@ -373,60 +374,66 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
     const int threads = ((ty * TZ + 31) / 32) * 32 + 32;
     const int regs_cta = threads * ((regs + 7) / 8 * 8);
     const int by_regs = 65536 / regs_cta;
-    const int64_t slot = ((T1 + 2 * H) * rowb0 + 128 + 127) / 128 * 128;
-    const int64_t smem_cta = 256 + NS * slot;
-    if (smem_cta > 220 * 1024) continue;
-    const int by_smem = (int)((228 * 1024) / (smem_cta + 1024));
-    const int ctas = std::min(by_regs, by_smem);
-    if (ctas < 1) continue;
-    // resident consumer threads, discounted by the halo re-read overhead
-    cands[ncand++] = {(double)ctas * ty * TZ * T1 / (T1 + 2.0 * H), ty};
+    const int slot = (T1 + 2 * H) * pitch;
+    for (int ctas = 1; ctas <= by_regs && ctas <= 4; ++ctas) {
+      const int per_cta = std::min(SMEM_SM / ctas - 1024, SMEM_CTA) - 256 - 128;
+      const int ns = std::min(NS_MAX, per_cta / slot);
+      if (ns < H + 3) continue;
+      const double cw = std::min(24.0, ctas * ((ty * TZ + 31) / 32.0));
+      const double eff = (double)T1 / (T1 + 2.0 * H);
+      const double pf = std::min(1.0, (ns - H - 1) / 4.0);
+      cands[ncand++] = {cw * eff * pf, ty, ctas, ns};
+    }
   }
   std::sort(cands, cands + ncand, [](const Cand& x, const Cand& y) { return x.score > y.score; });
-  int best_ty = -1, occ = 0, threads = 0;
-  size_t smem = 0;
-  for (int c = 0; c < ncand && best_ty < 0; ++c) {
-    const int ty = cands[c].ty;
-    const int T1 = ty * R1;
-    const int slotb = (int)((((T1 + 2 * H) * rowb0 + 128) + 127) / 128 * 128);
-    const size_t sm = 256 + (size_t)NS * slotb;
-    const int th = ((ty * TZ + 31) / 32) * 32 + 32;
+  int best = -1, occ = 0;
+  for (int c = 0; c < ncand && best < 0; ++c) {
+    const int th = ((cands[c].ty * TZ + 31) / 32) * 32 + 32;
+    const size_t sm = 256 + 128 + (size_t)cands[c].ns * (cands[c].ty * R1 + 2 * H) * pitch;
     int o = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, th, sm) == cudaSuccess && o >= 1) {
-      best_ty = ty; occ = o; threads = th; smem = sm;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, th, sm) == cudaSuccess && o >= cands[c].ctas) {
+      best = c;
+      occ = o;
     }
   }
   cudaGetLastError();
-  if (best_ty < 0) {
+  if (best < 0) {
     g_tma_reason = ncand ? "zero occupancy" : "no row tile fits the grid (periodic axis 1 needs T1 | n1)";
     return 1;
   }
+  const Cand cb = cands[best];
   TmaArgs a{};
-  a.out = out; a.y = ep.y; a.nbatch = nin;
+  a.out = out; a.y = ep.y; a.vpot = ep.vpot; a.nbatch = nin;
   a.n0 = n0; a.n1 = n1; a.n2 = n2;
   a.pbc0 = op->pbc[0]; a.pbc1 = op->pbc[1]; a.pbc2 = op->pbc[2];
-  a.TY = best_ty; a.TZ = TZ; a.NTC = best_ty * TZ; a.T1 = best_ty * R1; a.ROWS = a.T1 + 2 * H;
+  a.TY = cb.ty; a.TZ = TZ; a.NTC = cb.ty * TZ; a.T1 = cb.ty * R1; a.ROWS = a.T1 + 2 * H;
   a.ytiles = ceil_div(n1, a.T1);
-  const int64_t rowb = (int64_t)n2 * sizeof(T);
-  a.slot_bytes = (int)(((a.ROWS * rowb + 128) + 127) / 128 * 128);
+  a.NS = cb.ns;
+  a.pitch = pitch;
+  a.slot_bytes = a.ROWS * pitch;
   a.c0 = op->center;
   a.c0diff = op->center;
   for (int c = 0; c < 3; ++c)
     for (int m = 0; m < 2 * HMAX + 1; ++m) a.c0diff += op->a[c][m];
   memcpy(a.a, op->a, sizeof(a.a));
-  a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma; a.vpot = ep.vpot;
-  if (smem > 220 * 1024 || a.ROWS > 256) { g_tma_reason = "tile too large"; return 1; }
-  // tensor maps over (n2 scalars, n1, n0, nbatch)
+  a.c0f = (float)a.c0;
+  a.c0difff = (float)a.c0diff;
+  for (int c = 0; c < 3; ++c)
+    for (int m = 0; m < 2 * HMAX + 1; ++m) a.af[c][m] = (float)op->a[c][m];
+  a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma;
+  const size_t smem = 256 + 128 + (size_t)a.NS * a.slot_bytes;
+  // tensor maps over (n2 scalars, n1, n0, nbatch); the box spans the whole
+  // padded pitch, so the columns past n2 arrive as zeros
   const int scal = Elem<T>::cplx ? 2 : 1;
-  const CUtensorMapDataType dt = sizeof(typename Elem<T>::R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
-                                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-  const uint64_t es = sizeof(typename Elem<T>::R);
+  const CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const uint64_t es = sizeof(R);
   const uint64_t dims[4] = {(uint64_t)n2 * scal, (uint64_t)n1, (uint64_t)n0, (uint64_t)nin};
   const uint64_t strides[3] = {dims[0] * es, dims[0] * dims[1] * es, dims[0] * dims[1] * dims[2] * es};
+  const uint32_t bx = (uint32_t)(pitch / (int)es);
   CUtensorMap tmA, tmH, tmB;
-  const uint32_t boxA[4] = {(uint32_t)dims[0], (uint32_t)a.ROWS, 1, 1};
-  const uint32_t boxH[4] = {(uint32_t)dims[0], (uint32_t)H, 1, 1};
-  const uint32_t boxB[4] = {(uint32_t)dims[0], (uint32_t)(a.T1 + H), 1, 1};
+  const uint32_t boxA[4] = {bx, (uint32_t)a.ROWS, 1, 1};
+  const uint32_t boxH[4] = {bx, (uint32_t)H, 1, 1};
+  const uint32_t boxB[4] = {bx, (uint32_t)(a.T1 + H), 1, 1};
   void* base = const_cast<void*>(in);
   if (!encode_tensor_map_4d(&tmA, dt, base, dims, strides, boxA) ||
       !encode_tensor_map_4d(&tmH, dt, base, dims, strides, boxH) ||
@@ -434,8 +441,9 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
     g_tma_reason = "cuTensorMapEncodeTiled rejected the layout";
     return 1;
   }
+  const int threads = ((a.NTC + 31) / 32) * 32 + 32;
   const int64_t total = nin * (int64_t)a.ytiles * n0;
-  int64_t blocks = (int64_t)sm_count() * occ;
+  int64_t blocks = (int64_t)sm_count() * std::min(occ, cb.ctas);
   blocks = std::min<int64_t>(blocks, std::max<int64_t>(1, total / (4 * H + 4)));
   kern<<<(unsigned)blocks, threads, smem, st>>>(tmA, tmH, tmB, a);
   const int rc = check_launch("star_tma_kernel");
@@ -462,7 +470,7 @@ int star_tma_apply(const gb_operator* op, const void* in, void* out, int64_t nin
   }
   if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) { g_tma_reason = "unaligned data"; return 1; }
   if (ep.y && (reinterpret_cast<uintptr_t>(ep.y) & 15)) { g_tma_reason = "unaligned y"; return 1; }
-  if (op->n[0] < op->H || op->n[1] < op->H) { g_tma_reason = "grid shorter than the stencil"; return 1; }
+  if (op->n[0] < op->H || op->n[1] < op->H || op->n[2] < 8) { g_tma_reason = "grid shorter than the stencil"; return 1; }
   switch (dtype) {
     case GB_DTYPE_F64:
       switch (op->H) {
