@@ -49,6 +49,9 @@ _SIGNATURES = {
     'gb_transformer_apply': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,
                                      c_int, PD, c_void_p]),
     'gb_transformer_free': (c_int, [c_void_p]),
+    'gb_fd_precond_noalloc': (c_int, [c_void_p] * 7 + [c_void_p, c_void_p,
+                                                        c_double, c_int64, c_int,
+                                                        PD, c_void_p]),
     'gb_lfc_new': (c_int, [c_int, c_void_p, P64, c_void_p, c_void_p, c_int,
                            c_void_p, c_void_p, c_double, c_int, c_void_p,
                            c_int64, c_int, POINTER(c_void_p)]),

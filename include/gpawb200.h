@@ -132,6 +132,26 @@ int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* rest1,
                   double step, int64_t nin, int dtype,
                   const double* phase_cd, void* stream);
 
+/* The same V-cycle for callers that cannot allocate device memory while
+ * they run: a C or Fortran host program that owns only the residual and
+ * result buffers it passes in, or a process whose device-memory budget is
+ * fixed at start-up.  It has no counterpart in the reference.  The work grids
+ * come from one 64 MiB array inside the library (held by every GPU that
+ * loads it); a call needing more -- about 1.41 x nin x level-0 points x
+ * element size -- fails with GB_E_INVALID.  Nothing is allocated or freed.
+ * The first call on a device looks up the array's address: make it before
+ * any stream capture.  Calls share the array, so calls whose launches can
+ * overlap on the GPU race: keep them on one stream.  Result in d0, as
+ * gb_fd_precond. */
+int gb_fd_precond_noalloc(const gb_transformer* rest0,
+                          const gb_transformer* rest1,
+                          const gb_transformer* intp1,
+                          const gb_transformer* intp2,
+                          const gb_operator* kin0, const gb_operator* kin1,
+                          const gb_operator* kin2, void* d0,
+                          const void* residuals, double step, int64_t nin,
+                          int dtype, const double* phase_cd, void* stream);
+
 /* ======================================================================
  * Localized functions (LFC)  -- replaces _gpaw.LFC
  *   reference: c/lfc.c:146-257 (NewLFCObject), c/lfc.c:818-885 (add),
