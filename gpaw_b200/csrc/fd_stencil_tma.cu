@@ -134,7 +134,11 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
       tma_prefetch_desc(&tmH);
       tma_prefetch_desc(&tmB);
       const int tile_kind_first = a.pbc1 ? 1 : 0;
-      long long k = 0;
+      // ring position and the parity of the empty barrier to wait on (no wait
+      // during the first pass over the ring)
+      int slot = 0;
+      uint32_t eph = 0;
+      bool first_pass = true;
       int64_t s = s_begin;
       while (s < s_end) {
         const int64_t col = s / n0;
@@ -146,9 +150,8 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
         // 0: one box; 1: first tile of a periodic axis 1; 2: last tile of it
         const int kind = (tile_kind_first && y0 == 0) ? 1 : (a.pbc1 && y0 + T1 == n1) ? 2 : 0;
         const int L = p_end - p_start + 2 * H;
-        for (int t = 0; t < L; ++t, ++k) {
-          const int slot = (int)(k % NS);
-          if (k >= NS && !mbar_wait(&empty[slot], (uint32_t)(((k / NS) - 1) & 1))) {
+        for (int t = 0; t < L; ++t) {
+          if (!first_pass && !mbar_wait(&empty[slot], eph)) {
             raise_device_error(101);
             return;
           }
@@ -166,6 +169,11 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
           } else {
             tma_load_4d(dst, &tmB, &full[slot], 0, y0 - H, sp, band);
             tma_load_4d(dst + (T1 + H) * a.pitch, &tmH, &full[slot], 0, 0, sp, band);
+          }
+          if (++slot == NS) {
+            slot = 0;
+            if (first_pass) first_pass = false;
+            else eph ^= 1u;
           }
         }
       }
@@ -200,7 +208,8 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
   const R* __restrict__ vpot = reinterpret_cast<const R*>(a.vpot);
 
   T q[NQ][R1][R2];
-  long long k = 0;
+  int slot = 0;          // ring slot of the current step
+  uint32_t fph = 0;      // parity of its full barrier
   int64_t s = s_begin;
   while (s < s_end) {
     const int64_t col = s / n0;
@@ -219,9 +228,9 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
       for (int u = 0; u < NQ; ++u) {
         const int t = tb + u;
         if (t < L) {
-        const long long kk = k + t;
-        const int slot = (int)(kk % NS);
-        if (!mbar_wait(&full[slot], (uint32_t)((kk / NS) & 1))) {
+        int cslot = slot - H;  // slot of the centre plane (step t - H)
+        if (cslot < 0) cslot += NS;
+        if (!mbar_wait(&full[slot], fph)) {
           raise_device_error(102);
           return;
         }
@@ -233,7 +242,7 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
         if (t >= 2 * H) {
           const int cu = (u + NQ - H) % NQ;     // centre plane in the queue (static after unrolling)
           const int cpl = p_start + t - 2 * H;
-          const unsigned char* Pc = slots + (int64_t)((kk - H) % NS) * a.slot_bytes;
+          const unsigned char* Pc = slots + (int64_t)cslot * a.slot_bytes;
           T acc[R1][R2];
           // centre + axis 0 (register queue)
 #pragma unroll
@@ -326,17 +335,22 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
         // hand back the slot read as centre plane (its last reader was this step)
         if (t >= H) {
           __syncwarp();
-          if (lane == 0) mbar_arrive(&empty[(int)((kk - H) % NS)]);
+          if (lane == 0) mbar_arrive(&empty[cslot]);
+        }
+        if (++slot == NS) {
+          slot = 0;
+          fph ^= 1u;
         }
         }
       }
     }
     // segment end: release the slots of the last H planes (axis-0 neighbours only)
-    for (int t = L - H; t < L; ++t) {
+    for (int d = H; d >= 1; --d) {
+      int rs = slot - d;
+      if (rs < 0) rs += NS;
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[(int)((k + t) % NS)]);
+      if (lane == 0) mbar_arrive(&empty[rs]);
     }
-    k += L;
   }
 }
 
