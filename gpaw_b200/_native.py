@@ -67,6 +67,14 @@ _SIGNATURES = {
     'gb_conv3d_backward_weight': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,
                                           c_int, c_int, P64, POINTER(c_int),
                                           c_void_p]),
+    'gb_band_dots': (c_int, [c_int64, c_int64, c_void_p, c_int64, c_void_p,
+                             c_int64, c_int, c_void_p, c_void_p]),
+    'gb_band_gram': (c_int, [c_int64, c_int, c_int64, c_void_p, c_int64,
+                             c_int64, c_int, c_void_p, c_void_p]),
+    'gb_small_solve': (c_int, [c_int64, c_int, c_void_p, c_void_p, c_void_p,
+                               c_void_p, c_void_p]),
+    'gb_band_combine': (c_int, [c_int64, c_int64, c_int, c_void_p, c_void_p,
+                                c_void_p, c_void_p, c_int64, c_int, c_void_p]),
     'gb_xc_calculate': (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_void_p, c_void_p]),
     'gb_fd_precond': (c_int, [c_void_p] * 7 + [c_void_p] * 8 +

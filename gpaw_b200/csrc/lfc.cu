@@ -73,6 +73,7 @@ struct LfcView {
   const int* ct_nm;
   const int* ct_W;
   const int* gr_M;
+  const int* gr_nm;
   const int* gr_voff;
   const int* gv_W;
   const int64_t* vol_row0;
@@ -85,7 +86,7 @@ static LfcView view(const gb_lfc* l) {
   LfcView v;
   v.nW = l->nW; v.nM = l->nM; v.nG = l->nG; v.dv = l->dv; v.phase = l->phase;
   v.P = l->P; v.pt_G = l->pt_G; v.pt_off = l->pt_off; v.ct_aoff = l->ct_aoff;
-  v.ct_M = l->ct_M; v.ct_nm = l->ct_nm; v.ct_W = l->ct_W; v.gr_M = l->gr_M;
+  v.ct_M = l->ct_M; v.ct_nm = l->ct_nm; v.ct_W = l->ct_W; v.gr_M = l->gr_M; v.gr_nm = l->gr_nm;
   v.gr_voff = l->gr_voff; v.gv_W = l->gv_W; v.vol_row0 = l->vol_row0;
   v.vol_row1 = l->vol_row1; v.row_G = l->row_G; v.vol_aoff = l->vol_aoff;
   return v;
@@ -114,12 +115,16 @@ template <typename T> struct AType { using A = double; };
 template <> struct AType<float> { using A = float; };
 template <> struct AType<float2> { using A = float; };
 
-template <typename T, int XB>
-__global__ void lfc_add_kernel(const LfcView l, const typename AType<T>::A* __restrict__ A,
-                               const T* __restrict__ c_xM, T* __restrict__ a_xG, int64_t nx, int q) {
+// one thread per covered point and XB bands; a contribution's NMAX-padded A
+// row is loaded once and reused for every band (runtime nm <= NMAX)
+template <typename T, int XB, int NMAX>
+__global__ void __launch_bounds__(256) lfc_add_kernel(const LfcView l, const typename AType<T>::A* __restrict__ A,
+                                                      const T* __restrict__ c_xM, T* __restrict__ a_xG, int64_t nx,
+                                                      int q) {
   using R = typename Elem<T>::R;
   constexpr bool CPLX = Elem<T>::cplx;
   const int64_t x0 = (int64_t)blockIdx.y * XB;
+  const int nb = (int)(nx - x0 < XB ? nx - x0 : XB);
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < l.P; p += (int64_t)gridDim.x * blockDim.x) {
     const int G = l.pt_G[p];
     T acc[XB];
@@ -129,6 +134,9 @@ __global__ void lfc_add_kernel(const LfcView l, const typename AType<T>::A* __re
     for (int c = l.pt_off[p]; c < c1; ++c) {
       const typename AType<T>::A* Ar = A + l.ct_aoff[c];
       const int M = l.ct_M[c], nm = l.ct_nm[c];
+      R Av[NMAX];
+#pragma unroll
+      for (int m = 0; m < NMAX; ++m) Av[m] = m < nm ? (R)Ar[m] : (R)0;
       double pr = 1.0, pi = 0.0;
       if (CPLX && q >= 0) {
         const double2 ph = l.phase[(int64_t)q * l.nW + l.ct_W[c]];
@@ -136,23 +144,29 @@ __global__ void lfc_add_kernel(const LfcView l, const typename AType<T>::A* __re
       }
 #pragma unroll
       for (int i = 0; i < XB; ++i) {
-        if (x0 + i >= nx) break;
-        const T* cx = c_xM + (x0 + i) * l.nM + M;
-        T s = zero<T>();
-        for (int m = 0; m < nm; ++m) s = fmadd(s, (R)Ar[m], cx[m]);
-        acc[i] = add(acc[i], CPLX ? phase_mul(s, pr, pi) : s);
+        if (i < nb) {
+          const T* cx = c_xM + (x0 + i) * l.nM + M;
+          T s = zero<T>();
+#pragma unroll
+          for (int m = 0; m < NMAX; ++m)
+            if (m < nm) s = fmadd(s, Av[m], cx[m]);
+          acc[i] = add(acc[i], CPLX ? phase_mul(s, pr, pi) : s);
+        }
       }
     }
 #pragma unroll
     for (int i = 0; i < XB; ++i) {
-      if (x0 + i >= nx) break;
-      T* ap = a_xG + (x0 + i) * l.nG + G;
-      *ap = add(*ap, acc[i]);
+      if (i < nb) {
+        T* ap = a_xG + (x0 + i) * l.nG + G;
+        *ap = add(*ap, acc[i]);
+      }
     }
   }
 }
 
 // --------------------------------------------------------------- integrate
+// one CTA per (function group, XB bands); a group is one atom (all its
+// radial functions merged, nm <= NM of them) with all its periodic images
 template <typename T, int NM, int XB, int NT>
 __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, const typename AType<T>::A* __restrict__ A,
                                                           const T* __restrict__ a_xG, T* __restrict__ c_xM,
@@ -163,6 +177,7 @@ __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, cons
   const int g = group_base + blockIdx.x;
   const int64_t x0 = (int64_t)blockIdx.y * XB;
   const int M = l.gr_M[g];
+  const int nm = l.gr_nm[g];
   T acc[XB][NM];
 #pragma unroll
   for (int i = 0; i < XB; ++i)
@@ -177,28 +192,47 @@ __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, cons
       const double2 ph = l.phase[(int64_t)q * l.nW + W];
       pr = ph.x; pi = ph.y;
     }
-    T part[XB][NM];
+    if constexpr (!CPLX) {
+      // real data: every image has phase 1, accumulate straight into acc
+      for (int64_t r = r0 + threadIdx.x; r < r1; r += NT) {
+        const int G = l.row_G[r];
+        R Ar[NM];
 #pragma unroll
-    for (int i = 0; i < XB; ++i)
+        for (int m = 0; m < NM; ++m) Ar[m] = m < nm ? (R)AW[(r - r0) * nm + m] : (R)0;
 #pragma unroll
-      for (int m = 0; m < NM; ++m) part[i][m] = zero<T>();
-    for (int64_t r = r0 + threadIdx.x; r < r1; r += NT) {
-      const int G = l.row_G[r];
-      R Ar[NM];
+        for (int i = 0; i < XB; ++i) {
+          if (x0 + i < nx) {
+            const T v = a_xG[(x0 + i) * l.nG + G];
 #pragma unroll
-      for (int m = 0; m < NM; ++m) Ar[m] = (R)AW[(r - r0) * NM + m];
-#pragma unroll
-      for (int i = 0; i < XB; ++i) {
-        if (x0 + i >= nx) break;
-        const T v = a_xG[(x0 + i) * l.nG + G];
-#pragma unroll
-        for (int m = 0; m < NM; ++m) part[i][m] = fmadd(part[i][m], Ar[m], v);
+            for (int m = 0; m < NM; ++m) acc[i][m] = fmadd(acc[i][m], Ar[m], v);
+          }
+        }
       }
+    } else {
+      T part[XB][NM];
+#pragma unroll
+      for (int i = 0; i < XB; ++i)
+#pragma unroll
+        for (int m = 0; m < NM; ++m) part[i][m] = zero<T>();
+      for (int64_t r = r0 + threadIdx.x; r < r1; r += NT) {
+        const int G = l.row_G[r];
+        R Ar[NM];
+#pragma unroll
+        for (int m = 0; m < NM; ++m) Ar[m] = m < nm ? (R)AW[(r - r0) * nm + m] : (R)0;
+#pragma unroll
+        for (int i = 0; i < XB; ++i) {
+          if (x0 + i < nx) {
+            const T v = a_xG[(x0 + i) * l.nG + G];
+#pragma unroll
+            for (int m = 0; m < NM; ++m) part[i][m] = fmadd(part[i][m], Ar[m], v);
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < XB; ++i)
+#pragma unroll
+        for (int m = 0; m < NM; ++m) acc[i][m] = add(acc[i][m], phase_mul(part[i][m], pr, pi));
     }
-#pragma unroll
-    for (int i = 0; i < XB; ++i)
-#pragma unroll
-      for (int m = 0; m < NM; ++m) acc[i][m] = add(acc[i][m], CPLX ? phase_mul(part[i][m], pr, pi) : part[i][m]);
   }
   // block reduction: warp shuffles, then across warps
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -221,7 +255,7 @@ __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, cons
   __syncthreads();
   for (int e = threadIdx.x; e < XB * NM; e += NT) {
     const int i = e / NM, m = e % NM;
-    if (x0 + i >= nx) continue;
+    if (x0 + i >= nx || m >= nm) continue;
     T v = zero<T>();
     for (int w = 0; w < NT / 32; ++w) v = add(v, red[w][e]);
     T* cp = c_xM + (x0 + i) * l.nM + M + m;
@@ -232,7 +266,9 @@ __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, cons
 template <typename T, int NM>
 static int integrate_nm(const gb_lfc* l, int gbeg, int gcount, const void* a, void* c, int64_t nx, int q,
                         cudaStream_t st) {
-  constexpr int XB = NM <= 3 ? 8 : (NM <= 9 ? 4 : 2);
+  // accumulators per thread: XB x NM (twice that for complex images)
+  constexpr int XB0 = NM <= 2 ? 16 : (NM <= 4 ? 8 : (NM <= 8 ? 4 : (NM <= 16 ? 2 : 1)));
+  constexpr int XB = Elem<T>::cplx ? (XB0 >= 4 ? XB0 / 4 : 1) : XB0;
   constexpr int NT = 128;
   const typename AType<T>::A* A;
   if constexpr (std::is_same<typename AType<T>::A, float>::value) A = l->A32; else A = l->A64;
@@ -241,25 +277,31 @@ static int integrate_nm(const gb_lfc* l, int gbeg, int gcount, const void* a, vo
   return check_launch("lfc_integrate_kernel");
 }
 
+// smallest supported padded function count >= nm
+static int nm_class(int nm) {
+  for (int c : {1, 2, 4, 8, 16, 32, 64})
+    if (nm <= c) return c;
+  return 0;
+}
+
 template <typename T>
 static int integrate_t(const gb_lfc* l, const void* a, void* c, int64_t nx, int q, cudaStream_t st) {
-  // groups are sorted by nm on the host; launch one kernel per nm class
+  // groups are sorted by nm on the host; one launch per padded class
   int g = 0;
   while (g < l->ngroups) {
-    const int nm = l->h_gr_nm[g];
+    const int cls = nm_class(l->h_gr_nm[g]);
     int e = g;
-    while (e < l->ngroups && l->h_gr_nm[e] == nm) ++e;
+    while (e < l->ngroups && nm_class(l->h_gr_nm[e]) == cls) ++e;
     int rc;
-    switch (nm) {
+    switch (cls) {
       case 1: rc = integrate_nm<T, 1>(l, g, e - g, a, c, nx, q, st); break;
-      case 3: rc = integrate_nm<T, 3>(l, g, e - g, a, c, nx, q, st); break;
-      case 5: rc = integrate_nm<T, 5>(l, g, e - g, a, c, nx, q, st); break;
-      case 7: rc = integrate_nm<T, 7>(l, g, e - g, a, c, nx, q, st); break;
-      case 9: rc = integrate_nm<T, 9>(l, g, e - g, a, c, nx, q, st); break;
-      case 15: rc = integrate_nm<T, 15>(l, g, e - g, a, c, nx, q, st); break;
-      case 21: rc = integrate_nm<T, 21>(l, g, e - g, a, c, nx, q, st); break;
-      case 27: rc = integrate_nm<T, 27>(l, g, e - g, a, c, nx, q, st); break;
-      default: return fail(GB_E_UNSUPPORTED, "lfc: function count per radial function not in {1,3,5,7,9,15,21,27}");
+      case 2: rc = integrate_nm<T, 2>(l, g, e - g, a, c, nx, q, st); break;
+      case 4: rc = integrate_nm<T, 4>(l, g, e - g, a, c, nx, q, st); break;
+      case 8: rc = integrate_nm<T, 8>(l, g, e - g, a, c, nx, q, st); break;
+      case 16: rc = integrate_nm<T, 16>(l, g, e - g, a, c, nx, q, st); break;
+      case 32: rc = integrate_nm<T, 32>(l, g, e - g, a, c, nx, q, st); break;
+      case 64: rc = integrate_nm<T, 64>(l, g, e - g, a, c, nx, q, st); break;
+      default: return fail(GB_E_UNSUPPORTED, "lfc: more than 64 functions in one volume");
     }
     if (rc) return rc;
     g = e;
@@ -267,17 +309,30 @@ static int integrate_t(const gb_lfc* l, const void* a, void* c, int64_t nx, int 
   return GB_OK;
 }
 
-template <typename T>
-static int add_t(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st) {
-  constexpr int XB = 8;
-  if (l->P == 0) return GB_OK;
+template <typename T, int XB, int NMAX>
+static int add_nm(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st) {
   const typename AType<T>::A* A;
   if constexpr (std::is_same<typename AType<T>::A, float>::value) A = l->A32; else A = l->A64;
   const int NT = 256;
   const int64_t bx = std::min<int64_t>((l->P + NT - 1) / NT, (int64_t)sm_count() * 8);
   dim3 grid((unsigned)bx, (unsigned)((nx + XB - 1) / XB));
-  lfc_add_kernel<T, XB><<<grid, NT, 0, st>>>(view(l), A, (const T*)c, (T*)a, nx, q);
+  lfc_add_kernel<T, XB, NMAX><<<grid, NT, 0, st>>>(view(l), A, (const T*)c, (T*)a, nx, q);
   return check_launch("lfc_add_kernel");
+}
+
+template <typename T>
+static int add_t(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st) {
+  if (l->P == 0) return GB_OK;
+  switch (nm_class(l->maxnm)) {
+    case 1: return add_nm<T, 8, 1>(l, c, a, nx, q, st);
+    case 2: return add_nm<T, 8, 2>(l, c, a, nx, q, st);
+    case 4: return add_nm<T, 8, 4>(l, c, a, nx, q, st);
+    case 8: return add_nm<T, 8, 8>(l, c, a, nx, q, st);
+    case 16: return add_nm<T, 4, 16>(l, c, a, nx, q, st);
+    case 32: return add_nm<T, 2, 32>(l, c, a, nx, q, st);
+    case 64: return add_nm<T, 1, 64>(l, c, a, nx, q, st);
+    default: return fail(GB_E_UNSUPPORTED, "lfc: more than 64 functions in one volume");
+  }
 }
 
 static __global__ void to_float(const double* a, float* b, int64_t n) {

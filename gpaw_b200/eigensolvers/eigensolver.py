@@ -1,14 +1,21 @@
 """Eigensolver base: residuals and subspace diagonalisation
 (gpaw/eigensolvers/eigensolver.py:121-236) on the GPU.
 
-H_nn = dv psi^H (T + v) psi + P dH P^H is one GEMM plus small per-atom
-products; it is diagonalised in FP64 (torch.linalg.eigh on the device) and
-psi, (T + v) psi and P are rotated with GEMMs in the working precision.
+Projections are kept concatenated over atoms, P_nM (bands x sum_a ni_a),
+and the atomic Hamiltonian corrections as one block-diagonal dH_MM, so that
+sum_a p^a dH^a P^a is one GEMM and one LFC launch instead of a loop over
+atoms.  H_nn = dv psi^H (T + v) psi + P^* dH P^T is accumulated in FP64 and
+diagonalised in FP64 (torch.linalg.eigh on the device); psi, (T + v) psi and
+P are rotated with GEMMs in the working precision.  Eigenvalues stay on the
+device (kpt.eps_n, FP64), so an iteration needs no host round trip except
+the eigensolver of the subspace matrix itself.
 """
 from __future__ import annotations
 
 import numpy as np
 import torch
+
+from gpaw_b200.bandops import band_combine
 
 
 class Eigensolver:
@@ -23,53 +30,70 @@ class Eigensolver:
         self.preconditioner = preconditioner
 
     def iterate(self, ham, wfs):
-        error = 0.0
+        """One pass over the k-points; returns the eigenstate error as a
+        0-d FP64 device tensor (no host synchronisation)."""
+        error = None
         for kpt in wfs.kpt_u:
             if not wfs.orthonormalized:
                 wfs.orthonormalize(kpt)
-            weights = self.weights(kpt)
-            error += self.iterate_one_k_point(ham, wfs, kpt, weights)
+            e = self.iterate_one_k_point(ham, wfs, kpt, self.weights(kpt, wfs))
+            error = e if error is None else error + e
             wfs.orthonormalize(kpt)
         wfs.orthonormalized = True
         self.error = error
         return error
 
     @staticmethod
-    def weights(kpt):
+    def weights(kpt, wfs):
         """Occupied bands carry the k-point weight in the error sum (the
         reference's default 'occupied' band convergence)."""
-        w = np.where(np.asarray(kpt.f_n) > 0, kpt.weight, 0.0)
+        w = getattr(kpt, '_w_n', None)
+        if w is None:
+            w = torch.as_tensor(np.where(np.asarray(kpt.f_n) > 0, kpt.weight, 0.0),
+                                dtype=torch.float64, device=kpt.psit_nG.device)
+            kpt._w_n = w
         return w
 
-    def dH_times(self, wfs, ham, P_ani):
-        """C_ani = sum_j P_anj dH_aij (dS = 0 for norm-conserving setups)."""
-        return {a: P @ ham.dH_aii[a].to(P.dtype).T for a, P in P_ani.items()}
+    @staticmethod
+    def dH_times(ham, P_nM):
+        """C_nM = P_nM dH_MM^T (dS = 0 for norm-conserving setups)."""
+        return P_nM @ ham.dH_MM.to(P_nM.dtype).T
 
-    def calculate_residuals(self, kpt, wfs, ham, psit_nG, P_ani, eps_n, R_nG):
+    def calculate_residuals(self, kpt, wfs, ham, psit_nG, P_nM, eps_n, R_nG):
         """R = (T + v) psi - eps psi + sum_a p^a dH^a P^a
         (gpaw/eigensolvers/eigensolver.py:153-172)."""
-        eps = torch.as_tensor(np.asarray(eps_n), dtype=wfs.real_dtype,
-                              device=R_nG.device).reshape((-1, 1, 1, 1))
-        R_nG -= eps * psit_nG
-        C_ani = self.dH_times(wfs, ham, P_ani)
-        wfs.pt.add(R_nG, C_ani, kpt.q if wfs.dtype.is_complex else -1)
+        eps = eps_n.to(torch.float64)
+        band_combine(R_nG, torch.stack([torch.ones_like(eps), -eps], 1), [R_nG, psit_nG])
+        wfs.pt.add_M(R_nG, self.dH_times(ham, P_nM),
+                     kpt.q if wfs.dtype.is_complex else -1)
 
-    def subspace_diagonalize(self, ham, wfs, kpt):
+    def subspace_matrix(self, ham, wfs, kpt):
+        """(H_nn in FP64, (T + v) psi): everything before the eigensolver of
+        the subspace problem (no host synchronisation)."""
         psit = kpt.psit_nG
-        nb = psit.shape[0]
         Htpsit = torch.empty_like(psit)
         wfs.apply_pseudo_hamiltonian(kpt, ham, psit, Htpsit)
         H = wfs.matrix(psit, Htpsit)
         wide = torch.complex128 if wfs.dtype.is_complex else torch.float64
-        for a, P in kpt.P_ani.items():
-            Pw = P.to(wide)
-            H = H + Pw.conj() @ ham.dH_aii[a].to(wide) @ Pw.T
-        H64 = H
-        H64 = 0.5 * (H64 + H64.conj().T)
-        eps, V = torch.linalg.eigh(H64)
+        if kpt.P_nM is not None and kpt.P_nM.shape[-1]:
+            Pw = kpt.P_nM.to(wide)
+            H = H + (Pw.conj() @ ham.dH_MM.to(wide)) @ Pw.T
+        H = 0.5 * (H + H.conj().T)
+        return H, Htpsit
+
+    def subspace_rotate(self, wfs, kpt, eps, V, Htpsit):
+        """psi, (T + v) psi and P rotated to the eigenvectors V of H_nn."""
+        psit = kpt.psit_nG
+        nb = psit.shape[0]
         # phi_k = sum_m V[m, k] psi_m
         U = V.T.to(wfs.dtype)
         kpt.psit_nG = (U @ psit.reshape(nb, -1)).reshape(psit.shape)
         self.Htpsit_nG = (U @ Htpsit.reshape(nb, -1)).reshape(psit.shape)
-        kpt.P_ani = {a: U @ P for a, P in kpt.P_ani.items()}
-        kpt.eps_n = eps.cpu().numpy()
+        if kpt.P_nM is not None:
+            kpt.P_nM = U @ kpt.P_nM
+        kpt.eps_n = eps
+
+    def subspace_diagonalize(self, ham, wfs, kpt):
+        H, Htpsit = self.subspace_matrix(ham, wfs, kpt)
+        eps, V = torch.linalg.eigh(H)
+        self.subspace_rotate(wfs, kpt, eps, V, Htpsit)

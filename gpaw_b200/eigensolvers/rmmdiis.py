@@ -13,6 +13,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from gpaw_b200.bandops import band_combine, small_solve
 from gpaw_b200.eigensolvers.eigensolver import Eigensolver
 
 
@@ -30,29 +31,36 @@ class RMMDIIS(Eigensolver):
 
     def iterate_one_k_point(self, ham, wfs, kpt, weights):
         self.subspace_diagonalize(ham, wfs, kpt)
+        return self.update_bands(ham, wfs, kpt, weights)
+
+    def update_bands(self, ham, wfs, kpt, weights):
+        """Everything of one RMM-DIIS pass after the subspace rotation
+        (residuals, preconditioned steps, DIIS); returns the weighted
+        residual norm as a 0-d FP64 device tensor."""
         psit = kpt.psit_nG
         R = self.Htpsit_nG
-        q = kpt.q if wfs.dtype.is_complex else -1
-        self.calculate_residuals(kpt, wfs, ham, psit, kpt.P_ani, kpt.eps_n, R)
+        self.calculate_residuals(kpt, wfs, ham, psit, kpt.P_nM, kpt.eps_n, R)
         dv = wfs.gd.dv
         nb = psit.shape[0]
         B = nb if self.blocksize is None else self.blocksize
         Ht = lambda x, out: wfs.apply_pseudo_hamiltonian(kpt, ham, x, out)
 
         def dots(a, b):
-            # Re <a_n|b_n> per band
-            A = a.reshape(a.shape[0], -1)
-            Bm = b.reshape(b.shape[0], -1)
-            return (A.conj() * Bm).real.sum(dim=1, dtype=torch.float64) * dv
+            # Re <a_n|b_n> per band, FP64 accumulation
+            return wfs.band_dots(a, b) * dv
 
-        error = 0.0
+        def axpy(y, a_n, x):
+            # y_n += a_n x_n for every band, in place (one launch)
+            a_n = a_n.to(torch.float64).reshape(-1)
+            band_combine(y, torch.stack([torch.ones_like(a_n), a_n], 1), [y, x])
+
+        error = torch.zeros((), dtype=torch.float64, device=psit.device)
         for n1 in range(0, nb, B):
             n2 = min(n1 + B, nb)
             eps_x = kpt.eps_n[n1:n2]
             psitb = psit[n1:n2]
             Rb = R[n1:n2]
-            w = torch.as_tensor(weights[n1:n2], dtype=torch.float64, device=psit.device)
-            error += float((w * dots(Rb, Rb)).sum())
+            error = error + (weights[n1:n2] * dots(Rb, Rb)).sum()
             nbl = n2 - n1
             if self.niter > 1:
                 psit_diis = torch.empty((nbl, self.niter) + psit.shape[1:],
@@ -75,32 +83,32 @@ class RMMDIIS(Eigensolver):
                     lam = torch.where(lam.abs() > up, up * lam.sign(), lam)
                 else:
                     lam = lam.clamp(lo, up)
-            lam_b = lam.to(wfs.real_dtype).reshape(-1, 1, 1, 1)
-            psitb += lam_b * dpsit
-            Rb += lam_b * dR
+            axpy(psitb, lam, dpsit)
+            axpy(Rb, lam, dR)
             for nit in range(1, self.niter):
                 psit_diis[:, nit] = psitb
                 R_diis[:, nit] = Rb
                 if nit > 1 or self.limit_lambda:
-                    Rd = R_diis[:, :nit + 1].reshape(nbl, nit + 1, -1)
-                    R_nn = torch.einsum('bix,bjx->bij', Rd.conj(), Rd) * dv
+                    # R_ij = <R_i|R_j> over the stored residuals (one batched
+                    # Gram kernel), then the bordered DIIS system per band
+                    R_nn = wfs.band_gram(R_diis, nit + 1) * dv
                     A = -torch.ones((nbl, nit + 2, nit + 2), dtype=torch.float64,
                                     device=psit.device)
-                    A[:, :nit + 1, :nit + 1] = R_nn.real.to(torch.float64)
+                    A[:, :nit + 1, :nit + 1] = R_nn
                     A[:, -1, -1] = 0.0
                     x = torch.zeros((nbl, nit + 2), dtype=torch.float64, device=psit.device)
                     x[:, -1] = -1.0
-                    alpha = torch.linalg.solve(A, x)[:, :-1].to(wfs.real_dtype)
-                    al = alpha.reshape(nbl, nit + 1, 1, 1, 1)
-                    psitb.copy_((al * psit_diis[:, :nit + 1]).sum(1))
-                    Rb.copy_((al * R_diis[:, :nit + 1]).sum(1))
+                    alpha = small_solve(A, x)[0][:, :-1]
+                    band_combine(psitb, alpha, [psit_diis[:, i] for i in range(nit + 1)])
+                    band_combine(Rb, alpha, [R_diis[:, i] for i in range(nit + 1)])
                 if nit < self.niter - 1:
                     dpsit = self.preconditioner(Rb, kpt)
-                    psitb += lam_b * dpsit
+                    axpy(psitb, lam, dpsit)
                     Ht(psitb, Rb)
                     P = wfs.projections(psitb, kpt)
                     self.calculate_residuals(kpt, wfs, ham, psitb, P, eps_x, Rb)
             dpsit = self.preconditioner(Rb, kpt)
-            step = self.trial_step if self.trial_step is not None else lam_b
-            psitb += step * dpsit
+            step = (torch.full_like(lam, self.trial_step) if self.trial_step is not None
+                    else lam)
+            axpy(psitb, step, dpsit)
         return error

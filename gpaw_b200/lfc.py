@@ -64,6 +64,25 @@ def _box_functions(spline, beg_c, end_c, pos_v, gd, derivative=False):
     return A, G_b
 
 
+def _run_points(G_b):
+    """Grid point indices of the runs [G_b[0], G_b[1]), [G_b[2], G_b[3]), ..."""
+    return np.concatenate([np.arange(g0, g1) for g0, g1 in zip(G_b[0::2], G_b[1::2])]) \
+        if len(G_b) else np.zeros(0, np.int64)
+
+
+def _point_runs(G):
+    """Inverse of _run_points for a sorted index array."""
+    if len(G) == 0:
+        return np.zeros(0, np.intc)
+    brk = np.nonzero(np.diff(G) != 1)[0]
+    starts = np.concatenate([[0], brk + 1])
+    ends = np.concatenate([brk + 1, [len(G)]])
+    G_b = np.empty(2 * len(starts), np.intc)
+    G_b[0::2] = G[starts]
+    G_b[1::2] = G[ends - 1] + 1
+    return G_b
+
+
 class Sphere:
     def __init__(self, spline_j):
         self.spline_j = spline_j
@@ -220,16 +239,35 @@ class LocalizedFunctionsCollection(BaseLFC):
         if self.integral_a is not None:
             for a in self.atom_indices:
                 self.sphere_a[a].normalize(self.integral_a[a], self.gd.dv)
-        A_Wgm, M_W, sdisp_W, pos_W, G_list, W_list, box_W = [], [], [], [], [], [], []
+        # one device volume per (atom, periodic image): the radial functions
+        # of an atom are merged onto the union of their sphere points (zeros
+        # where a shorter function does not reach), so that add / integrate
+        # touch each covered grid point once per atom instead of once per
+        # radial function
+        A_Wgm, M_W, sdisp_W, G_list, W_list, box_W = [], [], [], [], [], []
         W = 0
         for a in self.atom_indices:
             s = self.sphere_a[a]
+            images = {}
             for A_gm, G_b, Mw, sd, box in zip(s.A_wgm, s.G_wb, s.M_w,
                                                s.sdisp_wc, s.box_w):
-                A_Wgm.append(A_gm)
-                M_W.append(self.M_a[a] + Mw)
-                sdisp_W.append(sd)
-                box_W.append((a,) + box)
+                images.setdefault(tuple(np.round(sd, 12)), []).append(
+                    (A_gm, _run_points(G_b), Mw, box))
+            for key, parts in images.items():
+                G = parts[0][1]
+                for part in parts[1:]:
+                    G = np.union1d(G, part[1])
+                A = np.zeros((len(G), s.Mmax))
+                members = []
+                for A_gm, Gp, Mw, box in parts:
+                    rows = np.searchsorted(G, Gp)
+                    A[rows, Mw:Mw + A_gm.shape[1]] = A_gm
+                    members.append((box, rows, Mw))
+                A_Wgm.append(A)
+                M_W.append(self.M_a[a])
+                sdisp_W.append(np.array(key))
+                box_W.append((a, len(G), members))
+                G_b = _point_runs(G)
                 G_list.append(G_b)
                 w = np.empty(len(G_b), np.intc)
                 w[0::2] = W
@@ -291,6 +329,18 @@ class LocalizedFunctionsCollection(BaseLFC):
             nat.dtype_code(a_xG), self._nq(a_xG, q), nat.stream_of(a_xG)),
             'gb_lfc_add')
 
+    def add_M(self, a_xG, c_xM, q=-1):
+        """add() with the coefficients already concatenated over atoms,
+        c_xM of shape xshape + (Mmax,) (no per-atom dict)."""
+        if self.Mmax == 0:
+            return
+        nx = int(np.prod(tuple(a_xG.shape[:-3]), dtype=np.int64))
+        c_xM = c_xM.to(a_xG.dtype).contiguous()
+        nat.check(nat.lib().gb_lfc_add(
+            self.lfc.handle, nat.ptr(c_xM), nat.ptr(a_xG), nx,
+            nat.dtype_code(a_xG), self._nq(a_xG, q), nat.stream_of(a_xG)),
+            'gb_lfc_add')
+
     def integrate(self, a_xG, c_axi, q=-1):
         """c_axi = dv sum_G a_xG Phi^a_i* (gpaw/lfc.py:552-631)."""
         nat.require_cuda(a_xG)
@@ -312,11 +362,15 @@ class LocalizedFunctionsCollection(BaseLFC):
     def _derivative_object(self):
         if self._deriv is None:
             dA_W = []
-            for (a, j, beg_c, end_c, pos_v) in self.box_W:
-                spline = self.sphere_a[a].spline_j[j]
-                dA, _ = _box_functions(spline, beg_c, end_c, pos_v, self.gd,
-                                       derivative=True)
-                dA_W.append(dA.reshape(dA.shape[0], -1))
+            for (a, ng, members) in self.box_W:
+                sphere = self.sphere_a[a]
+                dA = np.zeros((ng, 3 * sphere.Mmax))
+                for (j, beg_c, end_c, pos_v), rows, Mw in members:
+                    spline = sphere.spline_j[j]
+                    d, _ = _box_functions(spline, beg_c, end_c, pos_v, self.gd,
+                                          derivative=True)
+                    dA[rows, 3 * Mw:3 * Mw + d.shape[1] * 3] = d.reshape(d.shape[0], -1)
+                dA_W.append(dA)
             nG = int(np.prod(self.gd.n_c))
             self._deriv = _Native(dA_W, 3 * self.M_W, self.G_B, self.W_B,
                                   self.gd.dv, self.phase_qW, nG, 3 * self.Mmax)

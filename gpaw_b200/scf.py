@@ -31,6 +31,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
+from gpaw_b200.bandops import small_solve
 from gpaw_b200.grid_descriptor import GridDescriptor
 from gpaw_b200.hgh import HGHSetup
 from gpaw_b200.lfc import LFC
@@ -53,57 +54,76 @@ def h2gpts(h, cell_cv, idiv=4):
 
 class PulayMixer:
     """Pulay (DIIS) density mixing on the coarse grid (the role of
-    gpaw/mixer.py:35-; plain Euclidean metric)."""
+    gpaw/mixer.py:35-; plain Euclidean metric).
+
+    The last `nmaxold` input densities and residuals (raw, for the Pulay
+    matrix, and Kerker-filtered, for the update) live
+    in fixed ring buffers written at a device-side position, so once the
+    history is full a mixing step has fixed shapes and addresses and no host
+    synchronisation (it can be replayed inside a CUDA graph).  The Pulay
+    coefficients do not depend on the order of the history entries."""
 
     def __init__(self, beta=0.1, nmaxold=5, kerker_q0=None):
         self.beta = beta
         self.nmaxold = nmaxold
         self.kerker_q0 = kerker_q0
         self.gd = None
-        self.nin = []
-        self.res = []
+        self.reset()
 
     def _precondition(self, r_G):
         """Kerker filter k^2 / (k^2 + q0^2) on the residual (periodic cells):
         damps the long-wavelength charge sloshing of the density update."""
         if not self.kerker_q0 or self.gd is None:
             return r_G
-        gd = self.gd
-        ks = [2 * np.pi * np.fft.fftfreq(gd.N_c[c], gd.cell_cv[c, c] / gd.N_c[c])
-              for c in range(3)]
-        k2 = (ks[0][:, None, None]**2 + ks[1][None, :, None]**2 +
-              ks[2][None, None, :]**2)
-        f = torch.from_numpy(k2 / (k2 + self.kerker_q0**2)).to(r_G.device)
-        f[0, 0, 0] = 1.0
-        return torch.fft.ifftn(torch.fft.fftn(r_G) * f).real
+        if self._filter is None:
+            gd = self.gd
+            ks = [2 * np.pi * np.fft.fftfreq(gd.N_c[c], gd.cell_cv[c, c] / gd.N_c[c])
+                  for c in range(3)]
+            k2 = (ks[0][:, None, None]**2 + ks[1][None, :, None]**2 +
+                  ks[2][None, None, :]**2)
+            f = k2 / (k2 + self.kerker_q0**2)
+            f[0, 0, 0] = 1.0
+            self._filter = torch.from_numpy(f).to(r_G.device)
+        return torch.fft.ifftn(torch.fft.fftn(r_G) * self._filter).real
 
     def reset(self):
-        self.nin, self.res = [], []
+        self.count = 0
+        self.nin_h = None
+        self.res_h = None
+        self.pres_h = None
+        self.pos = None
+        self._filter = None
 
     def mix(self, nin_G, nout_G, dv):
-        self.nin.append(nin_G.clone())
-        self.res.append(nout_G - nin_G)
-        if len(self.nin) > self.nmaxold:
-            self.nin.pop(0)
-            self.res.pop(0)
-        m = len(self.res)
-        R = torch.stack([r.reshape(-1) for r in self.res])
-        A = (R @ R.T) * dv
+        if self.nin_h is None:
+            shape = (self.nmaxold,) + tuple(nin_G.shape)
+            self.nin_h = torch.zeros(shape, dtype=nin_G.dtype, device=nin_G.device)
+            self.res_h = torch.zeros_like(self.nin_h)
+            self.pres_h = torch.zeros_like(self.nin_h)
+            self.pos = torch.zeros(1, dtype=torch.int64, device=nin_G.device)
+        self.nin_h.index_copy_(0, self.pos, nin_G[None])
+        r_G = nout_G - nin_G
+        self.res_h.index_copy_(0, self.pos, r_G[None])
+        self.pres_h.index_copy_(0, self.pos, self._precondition(r_G)[None])
+        self.pos.add_(1).remainder_(self.nmaxold)
+        self.count = min(self.count + 1, self.nmaxold)
+        m = self.count
+        R = self.res_h[:m].reshape(m, -1)
         M = torch.zeros((m + 1, m + 1), dtype=torch.float64, device=R.device)
-        M[:m, :m] = A
+        M[:m, :m] = (R @ R.T) * dv
         M[:m, m] = 1.0
         M[m, :m] = 1.0
         rhs = torch.zeros(m + 1, dtype=torch.float64, device=R.device)
-        rhs[m] = 1.0
-        try:
-            alpha = torch.linalg.solve(M, rhs)[:m]
-        except RuntimeError:
-            alpha = torch.zeros(m, dtype=torch.float64, device=R.device)
-            alpha[-1] = 1.0
-        new = torch.zeros_like(nin_G)
-        for a, n, r in zip(alpha, self.nin, self.res):
-            new += a * (n + self.beta * self._precondition(r))
-        return new
+        rhs[m:].fill_(1.0)     # slice fill: a device kernel, no host copy
+        alpha, info = small_solve(M[None], rhs[None])
+        alpha, info = alpha[0, :m], info[0]
+        # a singular history falls back to the newest entry (no host check)
+        newest = torch.zeros_like(alpha)
+        newest.index_fill_(0, (self.pos - 1).remainder(self.nmaxold).clamp_max(m - 1), 1.0)
+        alpha = torch.where((info == 0) & torch.isfinite(alpha).all(), alpha, newest)
+        N = self.nin_h[:m].reshape(m, -1)
+        P = self.pres_h[:m].reshape(m, -1)
+        return (alpha.to(N.dtype) @ (N + self.beta * P)).reshape(nin_G.shape)
 
 
 @dataclass
@@ -115,6 +135,7 @@ class SCFLog:
     converged: bool = False
     iterations: int = 0
     wall: float = 0.0
+    graphed: bool = False
 
 
 class Calculation:
@@ -186,7 +207,7 @@ class Calculation:
         self.seed = seed
         self.k_c = np.zeros(3) if k_c is None else np.asarray(k_c, float)
         self.vHt_g = self.finegd.zeros()
-        self.dH_aii = None
+        self.dH_MM = None
         self._init_wavefunctions()
         self._init_density()
 
@@ -239,10 +260,9 @@ class Calculation:
     def update_hamiltonian(self):
         finegd = self.finegd
         nt_g = self.interpolator.apply(self.nt_G)
-        # renormalise the fine density to the electron count
-        Ntot = float(nt_g.sum()) * finegd.dv
-        if Ntot > 0:
-            nt_g *= self.nvalence / Ntot
+        # renormalise the fine density to the electron count (on the device)
+        Ntot = nt_g.sum() * finegd.dv
+        nt_g *= self.nvalence / Ntot.clamp_min(1e-300)
         rhot_g = nt_g + self.rhoion_g
         if self.pbc.all():
             rhot_g = rhot_g - rhot_g.mean()
@@ -250,54 +270,99 @@ class Calculation:
         vxc_g = torch.zeros((1,) + tuple(finegd.n_c), dtype=torch.float64,
                             device=finegd.device)
         e_g = finegd.empty()
-        Exc = self.xc.calculate(finegd, nt_g[None], vxc_g, e_g)
+        if self.xc.gd is not finegd:
+            self.xc.set_grid_descriptor(finegd)
+        self.xc.calculate_impl(finegd, nt_g[None], vxc_g, e_g)
+        Exc = e_g.sum() * finegd.dv
         vt_g = self.vbar_g + self.vHt_g + vxc_g[0]
-        self.vt_G = self.restrictor.apply(vt_g)
-        self.vt_G32 = self.vt_G.to(torch.float32)
-        self.dH_aii = {a: torch.from_numpy(s.dH_ii).to(self.gd.device)
-                       for a, s in enumerate(self.setups) if s.ni > 0}
-        self.e_hartree = 0.5 * float((rhot_g * self.vHt_g).sum()) * finegd.dv
-        self.e_xc = float(Exc)
-        self.e_vbar = float((nt_g * self.vbar_g).sum()) * finegd.dv
+        vt_G = self.restrictor.apply(vt_g)
+        # persistent state is updated in place (fixed addresses for replay)
+        if getattr(self, 'vt_G', None) is None:
+            self.vt_G = vt_G
+            self.vt_G32 = vt_G.to(torch.float32)
+        else:
+            self.vt_G.copy_(vt_G)
+            self.vt_G32.copy_(vt_G)
+        if self.dH_MM is None:
+            self.dH_MM = self._block_diagonal_dH()
+        # energy terms stay FP64 device scalars (read once per iteration)
+        e = torch.stack([0.5 * (rhot_g * self.vHt_g).sum() * finegd.dv, Exc,
+                         (nt_g * self.vbar_g).sum() * finegd.dv])
+        if getattr(self, 'e_terms', None) is None:
+            self.e_terms = e
+        else:
+            self.e_terms.copy_(e)
         self.nt_g = nt_g
         self.vt_g = vt_g
+
+    def _block_diagonal_dH(self):
+        """dH^a_ij of every atom on the diagonal of one (Mmax x Mmax) FP64
+        matrix, in the projector LFC's M order (the HGH dH_ij are
+        density-independent, so this is built once)."""
+        pt = self.wfs.pt
+        dH = torch.zeros((pt.Mmax, pt.Mmax), dtype=torch.float64)
+        for a, s in enumerate(self.setups):
+            if s.ni:
+                M = pt.M_a[a]
+                dH[M:M + s.ni, M:M + s.ni] = torch.from_numpy(np.asarray(s.dH_ii, float))
+        return dH.to(self.gd.device)
 
     def total_energy(self, kpt):
         """E = sum f eps - int nt vt + E_H + E_xc + E_vbar (Hartree),
         all sums in FP64 (the band energy counts kinetic + nonlocal +
         local parts of the input potential)."""
-        band = float(np.dot(kpt.f_n, kpt.eps_n))
-        nvt = float((self.nt_G * self.vt_G).sum()) * self.gd.dv
-        e_kin_nl = band - nvt
-        return e_kin_nl + self.e_hartree + self.e_xc + self.e_vbar
+        if getattr(kpt, '_f_t', None) is None:
+            kpt._f_t = torch.as_tensor(np.asarray(kpt.f_n, float), device=self.gd.device)
+        band = (kpt._f_t * kpt.eps_n).sum()
+        nvt = (self.nt_G * self.vt_G).sum() * self.gd.dv
+        return band - nvt + self.e_terms.sum()
 
     def update_density(self):
         nt_out = self.gd.zeros()
         for kpt in self.wfs.kpt_u:
             self.wfs.add_to_density(nt_out, kpt)
-        ddens = float((nt_out - self.nt_G).abs().sum()) * self.gd.dv / self.nvalence
-        self.nt_G = self.mixer.mix(self.nt_G, nt_out, self.gd.dv)
+        ddens = (nt_out - self.nt_G).abs().sum() * (self.gd.dv / self.nvalence)
+        self.nt_G.copy_(self.mixer.mix(self.nt_G, nt_out, self.gd.dv))
         self.nt_G.clamp_(min=0.0)
         return ddens
 
     # -------------------------------------------------------------- driver
+    def iteration(self):
+        """One SCF iteration, eagerly: RMM-DIIS pass, energy, density mixing,
+        new potential.  Returns the FP64 device vector [E (eV), eigenstate
+        error, density change]."""
+        kpt = self.wfs.kpt_u[0]
+        err = self.eigensolver.iterate(self, self.wfs)
+        E = self.total_energy(kpt) * Hartree
+        ddens = self.update_density()
+        self.update_hamiltonian()
+        return torch.stack([E, err, ddens])
+
     def run(self, maxiter=200, energy_tol=1e-5, density_tol=1e-4,
-            eigenstates_tol=4e-8, callback=None):
+            eigenstates_tol=4e-8, callback=None, graph=False):
         """Iterate to convergence: energy change (eV / valence electron)
         over the last 3 iterations < energy_tol, density change per
         electron < density_tol, eigenstate error (eV^2 / electron) <
-        eigenstates_tol."""
+        eigenstates_tol.
+
+        graph=True replays each iteration as two captured CUDA graphs (the
+        work before and after the subspace eigensolver, which runs eagerly
+        between them) once the mixer history is full; the first iterations
+        run eagerly.  Either way one iteration reads three scalars from the
+        device and nothing else."""
         log = SCFLog()
-        kpt = self.wfs.kpt_u[0]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         self.update_hamiltonian()
+        step = None
         for it in range(1, maxiter + 1):
-            err = self.eigensolver.iterate(self, self.wfs)
-            E = self.total_energy(kpt) * Hartree
-            ddens = self.update_density()
-            self.update_hamiltonian()
-            torch.cuda.synchronize()
+            if graph and it > self.mixer.nmaxold + 1:
+                if step is None:
+                    step = _GraphedIteration(self)
+                out = step.replay()
+            else:
+                out = self.iteration()
+            E, err, ddens = out.tolist()
             log.energies.append(E)
             log.errors.append(err * Hartree**2 / self.nvalence)
             log.ddens.append(ddens)
@@ -312,11 +377,16 @@ class Calculation:
                     log.converged = True
                     break
         log.wall = time.perf_counter() - t0
+        log.graphed = step is not None
+        if step is not None:
+            step.release()
         self.log = log
         return log
 
     def eigenvalues(self):
-        return np.asarray(self.wfs.kpt_u[0].eps_n) * Hartree
+        eps = self.wfs.kpt_u[0].eps_n
+        eps = eps.cpu().numpy() if isinstance(eps, torch.Tensor) else np.asarray(eps)
+        return eps * Hartree
 
 
 def si_diamond(ncell=1, a=5.43, rattle=0.0, seed=0):
@@ -341,3 +411,63 @@ def h2(vacuum=3.0, d=0.74):
     cell = [2 * vacuum, 2 * vacuum, 2 * vacuum + d]
     pos = np.array([[vacuum, vacuum, vacuum], [vacuum, vacuum, vacuum + d]])
     return ['H', 'H'], pos, cell
+
+
+class _GraphedIteration:
+    """One SCF iteration as two CUDA graphs around the subspace eigensolver.
+
+    Graph A: (T + v) psi and the FP64 subspace matrix H.  Then eigh(H) runs
+    eagerly (torch's eigh checks its info flag on the host) and writes into
+    fixed eigenvalue / eigenvector buffers.  Graph B: rotation, residuals,
+    the RMM-DIIS pass with its preconditioner calls, orthonormalisation,
+    energy, density and mixing, the new potential, and the copy of the new
+    wave functions and projections back into the buffers graph A reads.
+    Persistent SCF state (density, potential, energy terms, mixer history)
+    is updated in place by the eager code already, so its addresses do not
+    change between replays."""
+
+    def __init__(self, calc):
+        self.calc = calc
+        wfs = calc.wfs
+        kpt = wfs.kpt_u[0]
+        es = calc.eigensolver
+        weights = es.weights(kpt, wfs)
+        self.psit = kpt.psit_nG
+        self.P = kpt.P_nM
+        nb = self.psit.shape[0]
+        wide = torch.complex128 if wfs.dtype.is_complex else torch.float64
+        self.eps = torch.empty(nb, dtype=torch.float64, device=self.psit.device)
+        self.V = torch.empty((nb, nb), dtype=wide, device=self.psit.device)
+        self.pool = torch.cuda.graph_pool_handle()
+        torch.cuda.synchronize()
+        self.gA = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.gA, pool=self.pool):
+            self.H, self.Htpsit = es.subspace_matrix(calc, wfs, kpt)
+        self.gB = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.gB, pool=self.pool):
+            es.subspace_rotate(wfs, kpt, self.eps, self.V, self.Htpsit)
+            err = es.update_bands(calc, wfs, kpt, weights)
+            wfs.orthonormalize(kpt)
+            E = calc.total_energy(kpt) * Hartree
+            ddens = calc.update_density()
+            calc.update_hamiltonian()
+            self.psit.copy_(kpt.psit_nG)
+            if self.P is not None:
+                self.P.copy_(kpt.P_nM)
+            self.out = torch.stack([E, err, ddens])
+        kpt.psit_nG = self.psit
+        kpt.P_nM = self.P
+        kpt.eps_n = self.eps
+
+    def replay(self):
+        self.gA.replay()
+        eps, V = torch.linalg.eigh(self.H)
+        self.eps.copy_(eps)
+        self.V.copy_(V)
+        self.gB.replay()
+        return self.out
+
+    def release(self):
+        torch.cuda.synchronize()
+        self.gA.reset()
+        self.gB.reset()

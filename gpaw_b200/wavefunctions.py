@@ -16,6 +16,7 @@ import torch
 
 from gpaw_b200.fd_operators import Laplace
 from gpaw_b200.lfc import LFC
+from gpaw_b200.bandops import band_dots, band_gram
 
 REAL_OF = {torch.float64: torch.float64, torch.float32: torch.float32,
            torch.complex128: torch.float64, torch.complex64: torch.float32}
@@ -33,9 +34,9 @@ class KPoint:
         self.phase_cd = phase_cd
         self.weight = weight
         self.k_c = np.zeros(3) if k_c is None else np.asarray(k_c, float)
-        self.eps_n = None
+        self.eps_n = None     # FP64 device tensor after the first subspace step
         self.f_n = None
-        self.P_ani = {}
+        self.P_nM = None      # projections <p^a_i|psi_n>, concatenated over atoms
 
 
 class FDWaveFunctions:
@@ -62,10 +63,9 @@ class FDWaveFunctions:
         return Htpsit_xG
 
     def projections(self, psit_xG, kpt):
-        """P_ani = <p^a_i|psi_n> (LFC integrate, all bands at once)."""
-        c_axi = {}
-        cM = self.pt.integrate(psit_xG, c_axi, kpt.q if self.dtype.is_complex else -1)
-        return self.split_M(cM)
+        """P_xM = <p^a_i|psi_x>, concatenated over atoms (one LFC integrate
+        for all bands)."""
+        return self.pt.integrate(psit_xG, {}, kpt.q if self.dtype.is_complex else -1)
 
     def split_M(self, c_xM):
         return {a: c_xM[..., self.pt.M_a[a]:self.pt.M_a[a] + s.ni]
@@ -89,18 +89,28 @@ class FDWaveFunctions:
         S = self.matrix(psit, psit).to(torch.complex128 if self.dtype.is_complex
                                          else torch.float64)
         S = 0.5 * (S + S.conj().T)
-        L = torch.linalg.cholesky(S)
+        L = torch.linalg.cholesky_ex(S)[0]
         Linv = torch.linalg.solve_triangular(
             L, torch.eye(L.shape[0], dtype=L.dtype, device=L.device), upper=False)
         # psi_n <- sum_m Linv[n, m]^* psi_m  (S = L L^H, <phi|phi> = 1)
         C = Linv.conj().to(self.dtype)
         nb = psit.shape[0]
         kpt.psit_nG = (C @ psit.reshape(nb, -1)).reshape(psit.shape)
-        kpt.P_ani = self.projections(kpt.psit_nG, kpt)
+        kpt.P_nM = self.projections(kpt.psit_nG, kpt)
+
+    @staticmethod
+    def band_dots(a_nG, b_nG):
+        return band_dots(a_nG, b_nG)
+
+    @staticmethod
+    def band_gram(X_niG, k):
+        return band_gram(X_niG, k)
 
     def add_to_density(self, nt_G, kpt):
         from gpaw_b200 import _native as nat
-        f = torch.as_tensor(np.asarray(kpt.f_n, float), device=self.gd.device)
+        f = getattr(kpt, '_f_t', None)
+        if f is None:
+            f = kpt._f_t = torch.as_tensor(np.asarray(kpt.f_n, float), device=self.gd.device)
         nb = kpt.psit_nG.shape[0]
         nat.check(nat.lib().gb_add_to_density(
             nb, nat.ptr(f), nat.ptr(kpt.psit_nG), nat.dtype_code(kpt.psit_nG),

@@ -220,6 +220,35 @@ int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw,
                               const int64_t n_c[3], const int pbc_c[3],
                               void* stream);
 
+/* ======================================================================
+ * Per-band inner products of RMM-DIIS -- the gd.integrate(a_nG, b_nG) /
+ * np.dot calls of gpaw/eigensolvers/rmmdiis.py:133-145 (<R|R>, <dR|R>,
+ * <dR|dR>) and 175-190 (the DIIS matrix <R_i|R_j>), all bands per launch,
+ * FP64 accumulation for every storage dtype (no dv factor):
+ *   dots: out[n] = Re sum_G conj(a[n*lda + G]) b[n*ldb + G], G < N
+ *   gram: out[n][i][j] = Re sum_G conj(X[n*ldn + i*ldi + G]) X[n*ldn + j*ldi + G],
+ *         i, j < k <= 5
+ * ==================================================================== */
+int gb_band_dots(int64_t nb, int64_t N, const void* a, int64_t lda,
+                 const void* b, int64_t ldb, int dtype, double* out,
+                 void* stream);
+int gb_band_gram(int64_t nb, int k, int64_t N, const void* X, int64_t ldn,
+                 int64_t ldi, int dtype, double* out, void* stream);
+/* nb independent n x n FP64 systems A[s] x[s] = b[s] (n <= 8), the DIIS
+ * solves of gpaw/eigensolvers/rmmdiis.py:175-190 and of the density mixer
+ * (gpaw/mixer.py); partial pivoting; a singular system gives info[s] = 1 and
+ * x[s] = 0; no host synchronisation (info may be NULL). */
+int gb_small_solve(int64_t nb, int n, const double* A, const double* b,
+                   double* x, int* info, void* stream);
+/* Per-band linear combinations of RMM-DIIS (gpaw/eigensolvers/rmmdiis.py:
+ * 150-200: R -= eps psi, psi += lambda dpsi, the DIIS recombinations):
+ * out[n*ldo + G] = sum_{i<k} coef[n*k + i] x[i][n*ldx[i] + G], G < N, k <= 4,
+ * coef FP64 on the device; out may be one of the inputs.  x and ldx are host
+ * arrays of k entries. */
+int gb_band_combine(int64_t nb, int64_t N, int k, const double* coef,
+                    const void* const* x, const int64_t* ldx, void* out,
+                    int64_t ldo, int dtype, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
