@@ -13,8 +13,9 @@
 // accumulation FP32.  Boundaries per axis: zero padding or periodic wrap
 // (the grid's own boundary conditions).  Forward: a CTA stages a 1 x 4 x 32
 // point tile of all input channels plus halo in shared memory and every
-// thread produces all output channels of one point.  Backward-weight: one
-// CTA per (co, ci) pair owns its 27 sums (no atomics, deterministic).
+// thread produces all output channels of one point.  Backward-weight: CTAs
+// over (co, ci) pairs x chunks of the points; each reduces its chunk's 27
+// sums and adds them to dw with FP32 atomics (dw accumulates, as before).
 #include <cuda_bf16.h>
 #include <algorithm>
 #include "internal.cuh"
@@ -94,15 +95,19 @@ __global__ void __launch_bounds__(CT1 * CT2) conv3d_fwd_kernel(const ConvArgs a)
 }
 
 // dw[co][ci][k] += sum_b sum_p dy[b][co][p] x[b][ci][p + o_k]   (FP32)
+// grid: (cin * cout channel pairs) x (chunks of the band x point range);
+// each CTA reduces its chunk and adds its 27 sums to dw with atomics
 __global__ void __launch_bounds__(256) conv3d_bwd_w_kernel(const float* __restrict__ x, const float* __restrict__ dy,
                                                            float* __restrict__ dw, int64_t nb, int cin, int cout, int n0,
                                                            int n1, int n2, int pbc0, int pbc1, int pbc2) {
   const int co = blockIdx.x / cin, ci = blockIdx.x % cin;
   const int64_t n012 = (int64_t)n0 * n1 * n2;
+  const int64_t total = nb * n012;
+  const int64_t e0 = total * blockIdx.y / gridDim.y, e1 = total * (blockIdx.y + 1) / gridDim.y;
   float acc[27];
 #pragma unroll
   for (int k = 0; k < 27; ++k) acc[k] = 0.f;
-  for (int64_t e = threadIdx.x; e < nb * n012; e += blockDim.x) {
+  for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
     const int64_t b = e / n012, p = e % n012;
     const int g2 = (int)(p % n2), g1 = (int)((p / n2) % n1), g0 = (int)(p / ((int64_t)n1 * n2));
     const float d = dy[(b * cout + co) * n012 + p];
@@ -131,7 +136,7 @@ __global__ void __launch_bounds__(256) conv3d_bwd_w_kernel(const float* __restri
   if (threadIdx.x < 27) {
     float v = 0.f;
     for (int w = 0; w < (int)(blockDim.x / 32); ++w) v += red[w][threadIdx.x];
-    dw[((int64_t)co * cin + ci) * 27 + threadIdx.x] += v;
+    atomicAdd(&dw[((int64_t)co * cin + ci) * 27 + threadIdx.x], v);
   }
 }
 
@@ -174,7 +179,12 @@ int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw, int64_
   GB_REQUIRE(x && dy && dw && n_c && pbc_c && nb >= 0 && cin > 0 && cout > 0,
              "gb_conv3d_backward_weight: bad arguments");
   if (nb == 0) return GB_OK;
-  conv3d_bwd_w_kernel<<<cin * cout, 256, 0, (cudaStream_t)stream>>>(x, dy, dw, nb, cin, cout, (int)n_c[0],
+  // enough chunks to fill the GPU about four times over, each >= 4096 points
+  const int64_t total = nb * n_c[0] * n_c[1] * n_c[2];
+  const int64_t want = std::max<int64_t>(1, (int64_t)sm_count() * 8 / (cin * cout));
+  const int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(want, total / 4096));
+  dim3 grid((unsigned)(cin * cout), (unsigned)std::min<int64_t>(chunks, 65535));
+  conv3d_bwd_w_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(x, dy, dw, nb, cin, cout, (int)n_c[0],
                                                                     (int)n_c[1], (int)n_c[2], pbc_c[0], pbc_c[1],
                                                                     pbc_c[2]);
   return check_launch("conv3d_bwd_w_kernel");

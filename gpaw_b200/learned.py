@@ -10,7 +10,8 @@ V-cycle M(R) of gpaw/preconditioner.py inside RMM-DIIS:
     a2 = conv_b(r2)       16 -> 16     level 2
     u1 = Interp(a2) + a1               level 1
     b1 = conv_c(u1)       16 -> 1      level 1
-    y  = Interp(b1) + conv_0(x)  1->1  level 0
+    z  = Interp(b1)                    level 0
+    y  = conv_p(z) + conv_0(x)   1->1  level 0 (post- and pre-smoothing)
     out = s * y
 
 Convolutions are 3x3x3 with BF16 weights and FP32 accumulation
@@ -20,8 +21,13 @@ conv backward-weight = gb_conv3d_backward_weight; and the adjoints of the
 nn=1 transfer operators, Interp^T = 8 Restrict and Restrict^T = Interp / 8
 (exact for the linear-interpolation / full-weighting pair).  The network is
 linear and homogeneous of degree one in R, like M.  The loss is the mean
-over bands of ||out - M(R)||^2 / ||M(R)||^2 on (residual, multigrid
-correction) pairs that RMM-DIIS produces.
+over bands of ||A(out - M(R)/s)||^2 / ||A M(R)/s||^2 on (residual, multigrid
+correction) pairs that RMM-DIIS produces, in the energy norm A = K + 1
+(K = -1/2 nabla^2): an error e in a correction reappears as (K - eps) e in
+the next residual, so plain L2 would let high-frequency errors through that
+RMM-DIIS's fixed trial step amplifies.  s is the multigrid step of the grid
+(0.66666666 / diagonal of the kinetic stencil), which makes one set of
+weights serve grids of different spacing.
 
 At run time the multigrid preconditioner is both the fallback and the judge:
 every call compares the network with M on a few bands; if the relative
@@ -37,7 +43,8 @@ import torch
 from gpaw_b200 import _native as nat
 from gpaw_b200.transformers import Transformer
 
-SHAPES = {'w0': (1, 1, 27), 'wa': (16, 1, 27), 'wb': (16, 16, 27), 'wc': (1, 16, 27)}
+SHAPES = {'w0': (1, 1, 27), 'wa': (16, 1, 27), 'wb': (16, 16, 27), 'wc': (1, 16, 27),
+          'wp': (1, 1, 27)}
 
 
 def flip_transpose(w):
@@ -46,7 +53,7 @@ def flip_transpose(w):
 
 
 class ConvNet:
-    def __init__(self, gd0, seed=0, device=None):
+    def __init__(self, gd0, seed=0, device=None, params=None):
         self.gd0 = gd0
         self.gd1 = gd0.coarsen()
         self.gd2 = self.gd1.coarsen()
@@ -56,14 +63,74 @@ class ConvNet:
         self.r12 = Transformer(self.gd1, self.gd2, 1)
         self.i21 = Transformer(self.gd2, self.gd1, 1)
         self.i10 = Transformer(self.gd1, self.gd0, 1)
+        # energy-norm weight A = K + 1 (K = -1/2 nabla^2, 7-point, FP32):
+        # an error e in the correction costs ~ (K - eps) e in the next
+        # residual, so training and the judge measure errors through A
+        from gpaw_b200.fd_operators import Laplace
+        self.kin = Laplace(gd0, -0.5, 1, float)
+        if params is not None:
+            # the same weights on another grid (the network is translation
+            # invariant; only the transfer operators depend on the grid)
+            self.params = params
+            return
         g = torch.Generator().manual_seed(seed)
         self.params = {}
         for k, shp in SHAPES.items():
             fan_in = shp[1] * 27
-            self.params[k] = (torch.randn(shp, generator=g, dtype=torch.float64) /
-                              np.sqrt(fan_in)).to(torch.float32).to(self.device)
-        # start close to "identity-ish" smoothing: level-0 centre weight
-        self.params['w0'][0, 0, 13] = 0.5
+            w = torch.randn(shp, generator=g, dtype=torch.float64) / np.sqrt(fan_in)
+            if k == 'w0':
+                # start close to an identity-like smoother at level 0
+                w[0, 0, 13] = 0.5
+            if k == 'wp':
+                # the post-interpolation conv starts as the identity
+                w.zero_()
+                w[0, 0, 13] = 1.0
+            self.params[k] = w.to(torch.float32).to(self.device)
+
+    @staticmethod
+    def _stencil27(op):
+        """27-entry kernel of a radius-1 FD operator (entries of larger
+        offsets are dropped); index k <-> offset (k//9-1, (k//3)%3-1, k%3-1)."""
+        w = torch.zeros(27, dtype=torch.float64)
+        for c, o in zip(op.coef_p, np.asarray(op.offset_pc).reshape(-1, 3)):
+            if np.abs(o).max() <= 1:
+                w[(o[0] + 1) * 9 + (o[1] + 1) * 3 + (o[2] + 1)] += c
+        return w
+
+    def init_from_multigrid(self, mg):
+        """Set the weights to the V-cycle of `mg` (gpaw/preconditioner.py,
+        c/fd_preconditioner.c), in the network's normalised form T = M(R)/s:
+
+          a1: ch0 = -(4s K1 - 1) r1,  ch1 = -r1            (r1 = Restrict(x))
+          a2: ch2 = (32s - 256 s^2 K2) r2                  (r2 = Restrict(a1 ch0))
+          b1 = (8s - 16 s^2 K1) u1[ch1] + (4s K1 - 1) u1[ch2]
+          y  = (1/s - K0') Interp(b1) - x
+
+        K1, K2 are the 7-point coarse Laplacians of the V-cycle; K0' is the
+        radius-1 part of the fine kinetic stencil (the V-cycle's own K0 reaches
+        +-3 points, which a 3x3x3 kernel cannot hold -- training corrects it).
+        """
+        s = float(mg.step)
+        d = torch.zeros(27, dtype=torch.float64)
+        d[13] = 1.0
+        K1 = self._stencil27(mg.kin1)
+        K2 = self._stencil27(mg.kin2)
+        K0 = self._stencil27(mg.kin0)
+        w = {k: torch.zeros(shp, dtype=torch.float64) for k, shp in SHAPES.items()}
+        w['wa'][0, 0] = -(4 * s * K1 - d)
+        w['wa'][1, 0] = -d
+        w['wb'][2, 0] = 32 * s * d - 256 * s * s * K2
+        w['wc'][0, 1] = 8 * s * d - 16 * s * s * K1
+        w['wc'][0, 2] = 4 * s * K1 - d
+        w['wp'][0, 0] = d / s - K0
+        w['w0'][0, 0] = -d
+        for k in SHAPES:
+            self.params[k].copy_(w[k].to(self.params[k]))
+        return self
+
+    def on_grid(self, gd):
+        """This network (shared weights) on another grid descriptor."""
+        return ConvNet(gd, device=self.device, params=self.params)
 
     # -------------------------------------------------------------- kernels
     def _n(self, gd):
@@ -114,11 +181,12 @@ class ConvNet:
         a2 = self.conv(r2, p['wb'], self.gd2)                            # (nb, 16, n2)
         u1 = self.transfer(a2, self.i21) + a1                            # (nb, 16, n1)
         b1 = self.conv(u1, p['wc'], self.gd1)                            # (nb, 1, n1)
-        y = self.transfer(b1, self.i10)                                  # (nb, 1, n0)
+        z = self.transfer(b1, self.i10)                                  # (nb, 1, n0)
+        y = self.conv(z, p['wp'], self.gd0)
         self.conv(x, p['w0'], self.gd0, out=y, accumulate=True)
         out = y[:, 0] * s.reshape(-1, 1, 1, 1)
         if keep:
-            self._cache = dict(x=x, s=s, r1=r1, r2=r2, u1=u1)
+            self._cache = dict(x=x, s=s, r1=r1, r2=r2, u1=u1, z=z)
         return out
 
     def backward(self, g_out):
@@ -128,8 +196,10 @@ class ConvNet:
         p = self.params
         nb = g_out.shape[0]
         gy = (g_out * c['s'].reshape(-1, 1, 1, 1))[:, None].contiguous()   # (nb, 1, n0)
-        grads = {'w0': self.conv_bwd_w(c['x'], gy, p['w0'], self.gd0)}
-        gb1 = 8.0 * self.transfer(gy, self.r01)                             # Interp^T
+        grads = {'w0': self.conv_bwd_w(c['x'], gy, p['w0'], self.gd0),
+                 'wp': self.conv_bwd_w(c['z'], gy, p['wp'], self.gd0)}
+        gz = self.conv(gy, flip_transpose(p['wp']), self.gd0)               # (nb, 1, n0)
+        gb1 = 8.0 * self.transfer(gz, self.r01)                             # Interp^T
         grads['wc'] = self.conv_bwd_w(c['u1'], gb1, p['wc'], self.gd1)
         gu1 = self.conv(gb1, flip_transpose(p['wc']), self.gd1)            # (nb, 16, n1)
         ga2 = 8.0 * self.transfer(gu1, self.r12)                            # Interp^T
@@ -139,15 +209,22 @@ class ConvNet:
         grads['wa'] = self.conv_bwd_w(c['r1'], ga1, p['wa'], self.gd1)
         return grads
 
-    @staticmethod
-    def loss_and_grad(out, target):
-        """mean_b ||out_b - t_b||^2 / ||t_b||^2 and its gradient."""
+    def weight(self, x):
+        """A x = (K + 1) x for a batch (nb, n0, n1, n2) of FP32 grids."""
+        y = torch.empty_like(x)
+        self.kin.apply(x.contiguous(), y)
+        return y.add_(x)
+
+    def loss_and_grad(self, out, target):
+        """mean_b ||A(out_b - t_b)||^2 / ||A t_b||^2 and its gradient
+        2 A^T A (out - t) / (den nb) (A is symmetric)."""
         nb = out.shape[0]
         t = target.to(torch.float32)
         d = out - t
-        den = t.reshape(nb, -1).pow(2).sum(1).clamp_min(1e-30)
-        loss = (d.reshape(nb, -1).pow(2).sum(1) / den).mean()
-        g = 2.0 * d / (den.reshape(-1, 1, 1, 1) * nb)
+        Ad = self.weight(d)
+        den = self.weight(t).reshape(nb, -1).pow(2).sum(1).clamp_min(1e-30)
+        loss = (Ad.reshape(nb, -1).pow(2).sum(1) / den).mean()
+        g = 2.0 * self.weight(Ad) / (den.reshape(-1, 1, 1, 1) * nb)
         return float(loss), g
 
     # -------------------------------------------------------------- training
@@ -180,37 +257,137 @@ class ConvNet:
         return hist
 
     def relative_error(self, R, target):
+        """||net(R) - target|| / ||target|| per band (host array)."""
+        return self.relative_error_t(R, target).cpu().numpy()
+
+    def relative_error_from(self, out, target):
+        """||A(out - target)|| / ||A target|| per band (device tensor)."""
+        nb = out.shape[0]
+        t = target.to(torch.float32)
+        return (self.weight(out - t).reshape(nb, -1).norm(dim=1) /
+                self.weight(t).reshape(nb, -1).norm(dim=1).clamp_min(1e-30))
+
+    def relative_error_t(self, R, target):
         out = self.forward(R)
         nb = R.shape[0]
         t = target.to(torch.float32)
-        return ((out - t).reshape(nb, -1).norm(dim=1) / t.reshape(nb, -1).norm(dim=1)).cpu().numpy()
+        return (self.weight(out - t).reshape(nb, -1).norm(dim=1) /
+                self.weight(t).reshape(nb, -1).norm(dim=1).clamp_min(1e-30))
+
+
+def train_multi(sets, steps=400, lr=3e-3, batch=16, seed=0, log_every=0):
+    """Adam over several grids at once: `sets` is a list of (net, R, T)
+    with nets sharing one parameter dict (ConvNet.on_grid) and (R, T) the
+    (residual, scaled multigrid correction) pairs recorded on that net's
+    grid.  Each step takes a batch from one set, in proportion to its size.
+    Returns the loss history."""
+    params = sets[0][0].params
+    assert all(net.params is params for net, _, _ in sets)
+    m = {k: torch.zeros_like(v) for k, v in params.items()}
+    v2 = {k: torch.zeros_like(v) for k, v in params.items()}
+    b1, b2, eps = 0.9, 0.999, 1e-8
+    rng = np.random.default_rng(seed)
+    sizes = np.array([len(R) for _, R, _ in sets], float)
+    prob = sizes / sizes.sum()
+    hist = []
+    for it in range(1, steps + 1):
+        lr_t = lr * 0.5 * (1.0 + np.cos(np.pi * (it - 1) / steps))   # cosine decay
+        net, R_all, T_all = sets[rng.choice(len(sets), p=prob)]
+        idx = torch.as_tensor(rng.choice(len(R_all), size=min(batch, len(R_all)),
+                                         replace=False), device=R_all.device)
+        out = net.forward(R_all[idx].contiguous(), keep=True)
+        loss, g = net.loss_and_grad(out, T_all[idx].contiguous())
+        grads = net.backward(g)
+        for k in params:
+            m[k] = b1 * m[k] + (1 - b1) * grads[k]
+            v2[k] = b2 * v2[k] + (1 - b2) * grads[k]**2
+            params[k] -= lr_t * (m[k] / (1 - b1**it)) / ((v2[k] / (1 - b2**it)).sqrt() + eps)
+        hist.append(loss)
+        if log_every and it % log_every == 0:
+            print(f'  train step {it}: loss {np.mean(hist[-log_every:]):.4e}', flush=True)
+    return hist
+
+
+class PairRecorder:
+    """Wraps the multigrid preconditioner during ordinary iterations and
+    keeps (residual, correction / step) pairs of a few random bands per call:
+    the training data that the method itself generates."""
+
+    def __init__(self, multigrid, per_call=8, max_pairs=512, seed=0):
+        self.multigrid = multigrid
+        self.per_call = per_call
+        self.max_pairs = max_pairs
+        self.rng = np.random.default_rng(seed)
+        self.R = []
+        self.T = []
+        self.count = 0
+
+    def __call__(self, R, kpt=None, ekin=None, out=None):
+        y = self.multigrid(R, kpt, out=out)
+        if self.count < self.max_pairs and R.ndim == 4:
+            k = min(self.per_call, R.shape[0], self.max_pairs - self.count)
+            idx = torch.as_tensor(self.rng.choice(R.shape[0], size=k, replace=False),
+                                  device=R.device)
+            self.R.append(R[idx].to(torch.float32))
+            self.T.append((y[idx] / self.multigrid.step).to(torch.float32))
+            self.count += k
+        return y
+
+    def pairs(self):
+        return torch.cat(self.R), torch.cat(self.T)
 
 
 class LearnedPreconditioner:
-    """Drop-in for Preconditioner.__call__(R, kpt) with the multigrid as
-    fallback and judge."""
+    """Drop-in for Preconditioner.__call__(R, kpt): the network's correction
+    (scaled by the multigrid step of this grid), with the multigrid as judge
+    and fallback.
+
+    Every call also applies the multigrid to `nprobe` bands and compares; a
+    relative deviation above `tolerance` (or a non-finite output) sets the
+    device flag `failed`.  Nothing is read back during the call, so it runs
+    inside a captured SCF step; the SCF driver reads the flag once per
+    iteration with its other scalars and, when it is set, continues with the
+    multigrid alone (`fallback`)."""
 
     def __init__(self, net: ConvNet, multigrid, tolerance=0.5, nprobe=2):
         self.net = net
         self.multigrid = multigrid
+        self.fallback = multigrid
+        self.step = multigrid.step
         self.tolerance = tolerance
         self.nprobe = nprobe
-        self.calls = 0
-        self.fallbacks = 0
+        self.failed = torch.zeros((), dtype=torch.bool, device=net.device)
+        self.deviation = torch.zeros((), dtype=torch.float64, device=net.device)
 
     def __call__(self, R, kpt=None, ekin=None, out=None):
         if R.ndim == 3:
-            return self(R[None], kpt)[0]
-        self.calls += 1
-        y = self.net.forward(R).to(R.dtype)
+            o = None if out is None else out[None]
+            return self(R[None], kpt, out=o)[0]
+        yn = self.net.forward(R)
+        y = (yn * self.step).to(R.dtype)
         k = min(self.nprobe, R.shape[0])
-        probe = self.multigrid(R[:k].contiguous(), kpt)
-        dev = ((y[:k] - probe).reshape(k, -1).norm(dim=1) /
-               probe.reshape(k, -1).norm(dim=1).clamp_min(1e-30)).max().item()
-        if not np.isfinite(dev) or dev > self.tolerance:
-            self.fallbacks += 1
-            y = self.multigrid(R, kpt)
+        probe = (self.multigrid(R[:k].contiguous(), kpt) / self.step).to(torch.float32)
+        dev = self.net.relative_error_from(yn[:k], probe).max().to(torch.float64)
+        self.deviation.copy_(torch.maximum(self.deviation, dev))
+        bad = ~torch.isfinite(dev) | (dev > self.tolerance)
+        self.failed.logical_or_(bad)
         if out is not None:
             out.copy_(y)
             return out
         return y
+
+
+def collect_pairs(calc, iterations=6, per_call=8, max_pairs=512, seed=0):
+    """Run `iterations` ordinary SCF iterations of `calc` (eagerly, with its
+    multigrid preconditioner) and return the recorded (residual, correction /
+    step) pairs as two FP32 tensors (bands, n0, n1, n2)."""
+    mg = calc.preconditioner
+    rec = PairRecorder(mg, per_call=per_call, max_pairs=max_pairs, seed=seed)
+    calc.use_preconditioner(rec)
+    try:
+        calc.update_hamiltonian()
+        for _ in range(iterations):
+            calc.iteration()
+    finally:
+        calc.use_preconditioner(mg)
+    return rec.pairs()

@@ -136,6 +136,7 @@ class SCFLog:
     iterations: int = 0
     wall: float = 0.0
     graphed: bool = False
+    fallback_at: int = 0
 
 
 class Calculation:
@@ -336,7 +337,19 @@ class Calculation:
         E = self.total_energy(kpt) * Hartree
         ddens = self.update_density()
         self.update_hamiltonian()
-        return torch.stack([E, err, ddens])
+        return torch.stack([E, err, ddens, self._judge_flag()])
+
+    def _judge_flag(self):
+        """1.0 when a judged (learned) preconditioner has failed its check
+        against the multigrid, else 0.0 (a device scalar)."""
+        failed = getattr(self.preconditioner, 'failed', None)
+        if failed is None:
+            return torch.zeros((), dtype=torch.float64, device=self.gd.device)
+        return failed.to(torch.float64)
+
+    def use_preconditioner(self, pc):
+        self.preconditioner = pc
+        self.eigensolver.preconditioner = pc
 
     def run(self, maxiter=200, energy_tol=1e-5, density_tol=1e-4,
             eigenstates_tol=4e-8, callback=None, graph=False):
@@ -356,13 +369,21 @@ class Calculation:
         self.update_hamiltonian()
         step = None
         for it in range(1, maxiter + 1):
-            if graph and it > self.mixer.nmaxold + 1:
+            if graph and self.mixer.count == self.mixer.nmaxold:
                 if step is None:
                     step = _GraphedIteration(self)
                 out = step.replay()
             else:
                 out = self.iteration()
-            E, err, ddens = out.tolist()
+            E, err, ddens, failed = out.tolist()
+            if failed > 0.5:
+                # the multigrid judged the learned preconditioner off: go on
+                # with the multigrid (and capture the step again if graphed)
+                self.use_preconditioner(self.preconditioner.fallback)
+                log.fallback_at = it
+                if step is not None:
+                    step.release()
+                    step = None
             log.energies.append(E)
             log.errors.append(err * Hartree**2 / self.nvalence)
             log.ddens.append(ddens)
@@ -454,7 +475,7 @@ class _GraphedIteration:
             self.psit.copy_(kpt.psit_nG)
             if self.P is not None:
                 self.P.copy_(kpt.P_nM)
-            self.out = torch.stack([E, err, ddens])
+            self.out = torch.stack([E, err, ddens, calc._judge_flag()])
         kpt.psit_nG = self.psit
         kpt.P_nM = self.P
         kpt.eps_n = self.eps

@@ -77,15 +77,17 @@ class Net:
         a2 = conv(r2, p['wb'], pbc)
         u1 = self.T21.apply(a2) + a1
         b1 = conv(u1, p['wc'], pbc)
-        y = self.T10.apply(b1) + conv(x, p['w0'], pbc)
-        self.c = dict(x=x, s=s, r1=r1, r2=r2, u1=u1)
+        z = self.T10.apply(b1)
+        y = conv(z, p['wp'], pbc) + conv(x, p['w0'], pbc)
+        self.c = dict(x=x, s=s, r1=r1, r2=r2, u1=u1, z=z)
         return y[:, 0] * s[:, None, None, None]
 
     def backward(self, g):
         c, p, pbc = self.c, self.p, self.pbc
         gy = (g * c['s'][:, None, None, None])[:, None]
-        grads = {'w0': conv_bwd_w(c['x'], gy, pbc)}
-        gb1 = 8.0 * self.T01.apply(gy)
+        grads = {'w0': conv_bwd_w(c['x'], gy, pbc), 'wp': conv_bwd_w(c['z'], gy, pbc)}
+        gz = conv_bwd_x(gy, p['wp'], pbc)
+        gb1 = 8.0 * self.T01.apply(gz)
         grads['wc'] = conv_bwd_w(c['u1'], gb1, pbc)
         gu1 = conv_bwd_x(gb1, p['wc'], pbc)
         ga2 = 8.0 * self.T12.apply(gu1)
@@ -96,9 +98,18 @@ class Net:
         return grads
 
 
-def loss_and_grad(out, t):
+def weight(x, grid):
+    """A x = (K + 1) x, K = -1/2 nabla^2 with the 7-point (nn=1) stencil of
+    gpaw/fd_operators.py Laplace (the energy-norm weight of the loss)."""
+    coefs, offs = fd.guc_laplace(grid.h_cv, -0.5, 1)
+    return fd.fd_apply(coefs, offs, x, grid.pbc_c) + x
+
+
+def loss_and_grad(out, t, grid):
+    """mean_b ||A(out_b - t_b)||^2 / ||A t_b||^2 and its gradient
+    2 A^T A (out - t) / (den nb); A is symmetric."""
     nb = out.shape[0]
-    d = out - t
-    den = (t.reshape(nb, -1)**2).sum(1)
-    loss = ((d.reshape(nb, -1)**2).sum(1) / den).mean()
-    return loss, 2.0 * d / (den[:, None, None, None] * nb)
+    Ad = weight(out - t, grid)
+    den = (weight(t, grid).reshape(nb, -1)**2).sum(1)
+    loss = ((Ad.reshape(nb, -1)**2).sum(1) / den).mean()
+    return loss, 2.0 * weight(Ad, grid) / (den[:, None, None, None] * nb)

@@ -7,7 +7,8 @@ import pytest
 from oracle import fd
 from oracle import learned as ol
 
-SHAPES = {'w0': (1, 1, 27), 'wa': (16, 1, 27), 'wb': (16, 16, 27), 'wc': (1, 16, 27)}
+SHAPES = {'w0': (1, 1, 27), 'wa': (16, 1, 27), 'wb': (16, 16, 27), 'wc': (1, 16, 27),
+          'wp': (1, 1, 27)}
 
 
 @pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 0, 0)])
@@ -31,15 +32,15 @@ def test_oracle_gradient_vs_finite_differences(pbc):
     R = rng.standard_normal((2,) + tuple(g0.n_c))
     T = rng.standard_normal(R.shape)
     out = net.forward(R)
-    loss, g = ol.loss_and_grad(out, T)
+    loss, g = ol.loss_and_grad(out, T, g0)
     grads = net.backward(g)
     eps = 1e-6
     for k in SHAPES:
         for idx in [(0, 0, 13), (0, 0, 0), tuple(np.array(SHAPES[k]) - 1)]:
             p = {kk: v.copy() for kk, v in params.items()}
             p[k][idx] += eps
-            lp, _ = ol.loss_and_grad(ol.Net(g0, p).forward(R), T)
+            lp, _ = ol.loss_and_grad(ol.Net(g0, p).forward(R), T, g0)
             p[k][idx] -= 2 * eps
-            lm, _ = ol.loss_and_grad(ol.Net(g0, p).forward(R), T)
+            lm, _ = ol.loss_and_grad(ol.Net(g0, p).forward(R), T, g0)
             fdg = (lp - lm) / (2 * eps)
             assert abs(fdg - grads[k][idx]) < 1e-6 * max(1.0, abs(fdg)), (k, idx)
