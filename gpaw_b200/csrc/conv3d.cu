@@ -11,9 +11,11 @@
 //
 // Activations are FP32, weights BF16 (converted to FP32 in shared memory),
 // accumulation FP32.  Boundaries per axis: zero padding or periodic wrap
-// (the grid's own boundary conditions).  Forward: a CTA stages a 1 x 4 x 32
-// point tile of all input channels plus halo in shared memory and every
-// thread produces all output channels of one point.  Backward-weight: CTAs
+// (the grid's own boundary conditions).  Forward: a CTA covers 1 x 16 x 32
+// points; input channels are staged with their halo in shared memory four
+// at a time, the weights once, laid out [ci][k][co] so that four output
+// channels' weights come in one 16-byte broadcast load; every thread keeps
+// 4 consecutive points x all output channels in registers.  Backward-weight: CTAs
 // over (co, ci) pairs x chunks of the points; each reduces its chunk's 27
 // sums and adds them to dw with FP32 atomics (dw accumulates, as before).
 #include <cuda_bf16.h>
@@ -33,8 +35,12 @@ struct ConvArgs {
   int accumulate;           // y += conv(x) instead of y = conv(x)
 };
 
-constexpr int CT0 = 1, CT1 = 4, CT2 = 32;   // tile
-constexpr int HT0 = CT0 + 2, HT1 = CT1 + 2, HT2 = CT2 + 2;
+// forward tile: one plane (axis 0) x CY rows x CZ points; a thread owns PX
+// consecutive points of one row and all COUT outputs of them
+constexpr int CY = 16, CZ = 32, PX = 4;
+constexpr int CTHREADS = CY * (CZ / PX);            // 128
+constexpr int SY = CY + 2, SZP = 36;                 // staged rows, padded row pitch (floats)
+constexpr int CCH = 4;                               // input channels staged per pass
 
 __device__ __forceinline__ int cwrap(int i, int n) {
   int r = i % n;
@@ -42,54 +48,95 @@ __device__ __forceinline__ int cwrap(int i, int n) {
 }
 
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(CT1 * CT2) conv3d_fwd_kernel(const ConvArgs a) {
-  extern __shared__ float conv_smem[];
-  float (*sx)[HT0][HT1][HT2] = reinterpret_cast<float (*)[HT0][HT1][HT2]>(conv_smem);
-  float* sw = conv_smem + CIN * HT0 * HT1 * HT2;
+__global__ void __launch_bounds__(CTHREADS) conv3d_fwd_kernel(const ConvArgs a) {
+  constexpr int CC = CIN < CCH ? CIN : CCH;
+  extern __shared__ __align__(16) float conv_smem[];
+  float* sw = conv_smem;                               // [ci][k][co]
+  float* sx = conv_smem + ((CIN * 27 * COUT + 3) / 4) * 4;   // [cc][3][SY][SZP]
   const int tid = threadIdx.x;
-  for (int e = tid; e < COUT * CIN * 27; e += blockDim.x) sw[e] = __bfloat162float(a.w[e]);
-  const int t1n = (a.n1 + CT1 - 1) / CT1, t2n = (a.n2 + CT2 - 1) / CT2;
-  const int64_t ntile = (int64_t)a.n0 * t1n * t2n;
+  for (int e = tid; e < COUT * CIN * 27; e += CTHREADS) {
+    const int co = e / (CIN * 27), ci = (e / 27) % CIN, k = e % 27;
+    sw[(ci * 27 + k) * COUT + co] = __bfloat162float(a.w[e]);
+  }
+  const int tyn = (a.n1 + CY - 1) / CY, tzn = (a.n2 + CZ - 1) / CZ;
+  const int64_t ntile = (int64_t)a.n0 * tyn * tzn;
   const int64_t n012 = (int64_t)a.n0 * a.n1 * a.n2;
+  const int ty = tid / (CZ / PX), tz = (tid % (CZ / PX)) * PX;
   for (int64_t t = blockIdx.x; t < ntile * a.nb; t += gridDim.x) {
     const int64_t b = t / ntile;
     int64_t r = t % ntile;
-    const int i0 = (int)(r / (t1n * t2n));
-    r %= t1n * t2n;
-    const int j0 = (int)(r / t2n) * CT1, k0 = (int)(r % t2n) * CT2;
-    __syncthreads();
-    for (int e = tid; e < CIN * HT0 * HT1 * HT2; e += blockDim.x) {
-      const int kk = e % HT2, jj = (e / HT2) % HT1, ii = (e / (HT2 * HT1)) % HT0, ci = e / (HT2 * HT1 * HT0);
-      int g0 = i0 - 1 + ii, g1 = j0 - 1 + jj, g2 = k0 - 1 + kk;
-      float v = 0.f;
-      bool ok = true;
-      if (g0 < 0 || g0 >= a.n0) { if (a.pbc0) g0 = cwrap(g0, a.n0); else ok = false; }
-      if (g1 < 0 || g1 >= a.n1) { if (a.pbc1) g1 = cwrap(g1, a.n1); else ok = false; }
-      if (g2 < 0 || g2 >= a.n2) { if (a.pbc2) g2 = cwrap(g2, a.n2); else ok = false; }
-      if (ok) v = a.x[(b * CIN + ci) * n012 + ((int64_t)g0 * a.n1 + g1) * a.n2 + g2];
-      sx[ci][ii][jj][kk] = v;
-    }
-    __syncthreads();
-    const int tj = tid / CT2, tk = tid % CT2;
-    const int gj = j0 + tj, gk = k0 + tk;
-    if (gj >= a.n1 || gk >= a.n2) continue;
-    float acc[COUT];
+    const int i0 = (int)(r / (tyn * tzn));
+    r %= tyn * tzn;
+    const int j0 = (int)(r / tzn) * CY, k0 = (int)(r % tzn) * CZ;
+    float acc[PX][COUT];
 #pragma unroll
-    for (int co = 0; co < COUT; ++co) acc[co] = 0.f;
+    for (int p = 0; p < PX; ++p)
+#pragma unroll
+      for (int co = 0; co < COUT; ++co) acc[p][co] = 0.f;
+    for (int c0 = 0; c0 < CIN; c0 += CC) {
+      __syncthreads();   // previous pass (and the weight staging) done
+      for (int e = tid; e < CC * 3 * SY * (CZ + 2); e += CTHREADS) {
+        const int kk = e % (CZ + 2), jj = (e / (CZ + 2)) % SY, ii = (e / ((CZ + 2) * SY)) % 3;
+        const int cc = e / ((CZ + 2) * SY * 3);
+        int g0 = i0 - 1 + ii, g1 = j0 - 1 + jj, g2 = k0 - 1 + kk;
+        bool ok = true;
+        if (g0 < 0 || g0 >= a.n0) { if (a.pbc0) g0 = cwrap(g0, a.n0); else ok = false; }
+        if (g1 < 0 || g1 >= a.n1) { if (a.pbc1) g1 = cwrap(g1, a.n1); else ok = false; }
+        if (g2 < 0 || g2 >= a.n2) { if (a.pbc2) g2 = cwrap(g2, a.n2); else ok = false; }
+        sx[((cc * 3 + ii) * SY + jj) * SZP + kk] =
+            ok ? a.x[(b * CIN + c0 + cc) * n012 + ((int64_t)g0 * a.n1 + g1) * a.n2 + g2] : 0.f;
+      }
+      __syncthreads();
 #pragma unroll 1
-    for (int ci = 0; ci < CIN; ++ci) {
+      for (int cc = 0; cc < CC; ++cc) {
+        const float* wc = sw + (c0 + cc) * 27 * COUT;
 #pragma unroll
-      for (int k = 0; k < 27; ++k) {
-        const float v = sx[ci][k / 9][tj + (k / 3) % 3][tk + k % 3];
+        for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-        for (int co = 0; co < COUT; ++co) acc[co] = fmaf(sw[(co * CIN + ci) * 27 + k], v, acc[co]);
+          for (int dy = 0; dy < 3; ++dy) {
+            const float* row = sx + ((cc * 3 + dx) * SY + ty + dy) * SZP + tz;
+            float in[PX + 2];
+            const float4 v4 = *reinterpret_cast<const float4*>(row);
+            in[0] = v4.x; in[1] = v4.y; in[2] = v4.z; in[3] = v4.w;
+            in[4] = row[4]; in[5] = row[5];
+#pragma unroll
+            for (int dz = 0; dz < 3; ++dz) {
+              const float* wk = wc + (dx * 9 + dy * 3 + dz) * COUT;
+              if constexpr (COUT % 4 == 0) {
+#pragma unroll
+                for (int co = 0; co < COUT; co += 4) {
+                  const float4 w4 = *reinterpret_cast<const float4*>(wk + co);
+#pragma unroll
+                  for (int p = 0; p < PX; ++p) {
+                    acc[p][co] = fmaf(w4.x, in[p + dz], acc[p][co]);
+                    acc[p][co + 1] = fmaf(w4.y, in[p + dz], acc[p][co + 1]);
+                    acc[p][co + 2] = fmaf(w4.z, in[p + dz], acc[p][co + 2]);
+                    acc[p][co + 3] = fmaf(w4.w, in[p + dz], acc[p][co + 3]);
+                  }
+                }
+              } else {
+#pragma unroll
+                for (int co = 0; co < COUT; ++co) {
+                  const float w = wk[co];
+#pragma unroll
+                  for (int p = 0; p < PX; ++p) acc[p][co] = fmaf(w, in[p + dz], acc[p][co]);
+                }
+              }
+            }
+          }
       }
     }
-    const int64_t p = ((int64_t)i0 * a.n1 + gj) * a.n2 + gk;
+    const int gj = j0 + ty;
+    if (gj < a.n1) {
 #pragma unroll
-    for (int co = 0; co < COUT; ++co) {
-      float* yp = a.y + (b * COUT + co) * n012 + p;
-      *yp = a.accumulate ? *yp + acc[co] : acc[co];
+      for (int co = 0; co < COUT; ++co) {
+        float* yp = a.y + (b * COUT + co) * n012 + ((int64_t)i0 * a.n1 + gj) * a.n2;
+#pragma unroll
+        for (int p = 0; p < PX; ++p) {
+          const int gk = k0 + tz + p;
+          if (gk < a.n2) yp[gk] = a.accumulate ? yp[gk] + acc[p][co] : acc[p][co];
+        }
+      }
     }
   }
 }
@@ -142,15 +189,18 @@ __global__ void __launch_bounds__(256) conv3d_bwd_w_kernel(const float* __restri
 
 template <int CIN, int COUT>
 static int fwd_launch(const ConvArgs& a, cudaStream_t st) {
-  const int64_t tiles = (int64_t)a.n0 * ((a.n1 + CT1 - 1) / CT1) * ((a.n2 + CT2 - 1) / CT2) * a.nb;
-  const int64_t blocks = std::min<int64_t>(tiles, (int64_t)sm_count() * 8);
-  const size_t smem = (size_t)(CIN * HT0 * HT1 * HT2 + COUT * CIN * 27) * sizeof(float);
+  constexpr int CC = CIN < CCH ? CIN : CCH;
+  const int64_t tiles = (int64_t)a.n0 * ((a.n1 + CY - 1) / CY) * ((a.n2 + CZ - 1) / CZ) * a.nb;
+  const size_t smem = (size_t)(((CIN * 27 * COUT + 3) / 4) * 4 + CC * 3 * SY * SZP) * sizeof(float);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(conv3d_fwd_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
-  conv3d_fwd_kernel<CIN, COUT><<<(unsigned)std::max<int64_t>(blocks, 1), CT1 * CT2, smem, st>>>(a);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3d_fwd_kernel<CIN, COUT>, CTHREADS, smem);
+  const int64_t blocks = std::min<int64_t>(tiles, (int64_t)sm_count() * std::max(per_sm, 1) * 2);
+  conv3d_fwd_kernel<CIN, COUT><<<(unsigned)std::max<int64_t>(blocks, 1), CTHREADS, smem, st>>>(a);
   return check_launch("conv3d_fwd_kernel");
 }
 

@@ -91,13 +91,31 @@ __device__ __forceinline__ R coef(const TmaArgs& a, int c, int m) {
 // out-of-bounds fill (zeros); on a zero-boundary axis 2 the pitch keeps at
 // least 16 such bytes, and the halo chunks left of column 0 / right of column
 // n2 - 1 read them, so the consumers have no boundary branches at all.
-template <typename T, int H, int R1, int R2>
+// shared-memory vector loads of VB bytes (16: float4, 8: float2)
+template <typename T, int N, int VB>
+__device__ __forceinline__ void ldv(const T* p, T (&v)[N]) {
+  if constexpr (VB == 16) {
+    lds_vec<T, N>(p, v);
+  } else {
+    constexpr int V = 8 / (int)sizeof(T);
+    static_assert(N % V == 0, "");
+#pragma unroll
+    for (int i = 0; i < N / V; ++i) {
+      const float2 x = *reinterpret_cast<const float2*>(p + i * V);
+      const T* e = reinterpret_cast<const T*>(&x);
+#pragma unroll
+      for (int k = 0; k < V; ++k) v[i * V + k] = e[k];
+    }
+  }
+}
+
+template <typename T, int H, int R1, int R2, int VB>
 __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                         const __grid_constant__ CUtensorMap tmH,
                                                         const __grid_constant__ CUtensorMap tmB,
                                                         const __grid_constant__ TmaArgs a) {
   using R = typename Elem<T>::R;
-  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int VEC = VB / (int)sizeof(T);   // elements per vector access
   constexpr int HZ = ((H + VEC - 1) / VEC) * VEC;
   constexpr int NQ = 2 * H + 1;
   static_assert(R2 % VEC == 0, "");
@@ -237,7 +255,7 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
         const unsigned char* P = slots + (int64_t)slot * a.slot_bytes;
 #pragma unroll
         for (int r = 0; r < R1; ++r)
-          lds_vec<T, R2>(reinterpret_cast<const T*>(P + own_row + r * pitch + own_col), q[u][r]);
+          ldv<T, R2, VB>(reinterpret_cast<const T*>(P + own_row + r * pitch + own_col), q[u][r]);
 
         if (t >= 2 * H) {
           const int cu = (u + NQ - H) % NQ;     // centre plane in the queue (static after unrolling)
@@ -266,8 +284,8 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
 #pragma unroll
             for (int ch = 0; ch < HZ / VEC; ++ch) {
               T tl[VEC], tr[VEC];
-              lds_vec<T, VEC>(reinterpret_cast<const T*>(Pc + lcol[ch] + r * pitch), tl);
-              lds_vec<T, VEC>(reinterpret_cast<const T*>(Pc + rcol[ch] + r * pitch), tr);
+              ldv<T, VEC, VB>(reinterpret_cast<const T*>(Pc + lcol[ch] + r * pitch), tl);
+              ldv<T, VEC, VB>(reinterpret_cast<const T*>(Pc + rcol[ch] + r * pitch), tr);
 #pragma unroll
               for (int v = 0; v < VEC; ++v) {
                 wl[ch * VEC + v] = tl[v];
@@ -294,7 +312,7 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
 #pragma unroll
               for (int c = 0; c < R2; ++c) v[c] = q[cu][rr][c];
             } else {
-              lds_vec<T, R2>(reinterpret_cast<const T*>(Pc + own_row + rr * pitch + own_col), v);
+              ldv<T, R2, VB>(reinterpret_cast<const T*>(Pc + own_row + rr * pitch + own_col), v);
             }
 #pragma unroll
             for (int r = 0; r < R1; ++r) {
@@ -323,11 +341,19 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
               }
 #pragma unroll
               for (int c = 0; c < R2; c += VEC) {
-                float4 w4;
-                T* e = reinterpret_cast<T*>(&w4);
+                if constexpr (VB == 16) {
+                  float4 w4;
+                  T* e = reinterpret_cast<T*>(&w4);
 #pragma unroll
-                for (int v = 0; v < VEC; ++v) e[v] = acc[r][c + v];
-                __stcs(reinterpret_cast<float4*>(dst + p + c), w4);
+                  for (int v = 0; v < VEC; ++v) e[v] = acc[r][c + v];
+                  __stcs(reinterpret_cast<float4*>(dst + p + c), w4);
+                } else {
+                  float2 w2;
+                  T* e = reinterpret_cast<T*>(&w2);
+#pragma unroll
+                  for (int v = 0; v < VEC; ++v) e[v] = acc[r][c + v];
+                  __stcs(reinterpret_cast<float2*>(dst + p + c), w2);
+                }
               }
             }
           }
@@ -355,13 +381,13 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
 }
 
 // ------------------------------------------------------------------ host
-template <typename T, int H, int R1, int R2>
+template <typename T, int H, int R1, int R2, int VB = 16>
 static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int64_t nin, cudaStream_t st,
                           const Epilogue& ep) {
   using R = typename Elem<T>::R;
   const int n0 = (int)op->n[0], n1 = (int)op->n[1], n2 = (int)op->n[2];
   const int TZ = n2 / R2;
-  auto kern = star_tma_kernel<T, H, R1, R2>;
+  auto kern = star_tma_kernel<T, H, R1, R2, VB>;
   static int regs = -1;
   if (regs < 0) {
     cudaFuncAttributes fa;

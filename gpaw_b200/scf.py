@@ -144,12 +144,13 @@ class Calculation:
 
     symbols, positions (Angstrom), cell (Angstrom, 3 or 3x3), pbc;
     h (Angstrom), nbands, xc ('LDA' or 'PBE'), precision 'fp64' | 'fp32',
-    preconditioner None (multigrid) or an object with __call__(R, kpt)."""
+    preconditioner None (multigrid) or an object with __call__(R, kpt),
+    blocksize: RMM-DIIS band block (None = all bands per launch)."""
 
     def __init__(self, symbols, positions, cell, pbc, h=0.2, nbands=None,
                  xc='LDA', precision='fp64', k_c=None, preconditioner=None,
                  mixer_beta=None, seed=0, device='cuda', stencil=3,
-                 r_gauss=0.6, kerker_q0=1.0):
+                 r_gauss=0.6, kerker_q0=1.0, blocksize=None):
         cell = np.array(cell, float)
         cell_cv = np.diag(cell) if cell.ndim == 1 else cell
         self.cell_cv = cell_cv / Bohr
@@ -201,7 +202,9 @@ class Calculation:
         self.mixer = PulayMixer(beta=mixer_beta or (0.25 if periodic else 0.25),
                                 kerker_q0=kerker_q0 if periodic else None)
         self.mixer.gd = self.gd
-        self.eigensolver = RMMDIIS()
+        # blocksize None: every band in every launch (the batched form);
+        # 10: the reference's default RMM-DIIS band blocks
+        self.eigensolver = RMMDIIS(blocksize=blocksize)
         self.preconditioner = preconditioner or Preconditioner(
             self.gd, self.wfs.kin, complex if cplx else float, block=10)
         self.eigensolver.initialize(self.wfs, self.preconditioner)
