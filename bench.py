@@ -422,7 +422,12 @@ def main():
     ap.add_argument('--kernel-only', action='store_true',
                     help='time the stencil step only (no e2e, suite or CPU '
                          'baseline): the command line used for ncu captures')
+    ap.add_argument('--dtype', default='f64', choices=['f64', 'f32'],
+                    help='storage precision of the kernel-only run (the '
+                         'benchmark line itself is FP64)')
     args = ap.parse_args()
+    if args.dtype != 'f64' and not args.kernel_only:
+        ap.error('--dtype f32 is for --kernel-only runs; the benchmark line is FP64')
     if args.impl == 'reference':
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count() or 1))
         run_reference(args)
@@ -446,19 +451,22 @@ def main():
     lap = Laplace(gd, -0.5, 3)
     g = torch.Generator(device='cuda').manual_seed(0)
     nb = args.bands
-    x = torch.randn((nb, N, N, N), generator=g, device='cuda', dtype=torch.float64)
+    tdt = torch.float64 if args.dtype == 'f64' else torch.float32
+    cname = 'double' if args.dtype == 'f64' else 'float'
+    x = torch.randn((nb, N, N, N), generator=g, device='cuda', dtype=tdt)
     y = torch.empty_like(x)
-    nbytes = 2 * x.numel() * 8
+    nbytes = 2 * x.numel() * x.element_size()
     # which stencil kernel serves this layout: try the TMA pipeline alone
     nat.check(nat.lib().gb_set_stencil_path(2), 'stencil path')
     try:
         lap.apply(x[:1], y[:1])
-        kernel = 'star_tma_kernel<double,H=3,R1=2,R2=2>'
+        kernel = (f'star_tma_kernel<{cname},H=3,R1=2,R2=2>' if args.dtype == 'f64'
+                  else f'star_tma_kernel<{cname},H=3,R1=2,R2=4>')
     except nat.GPAWB200Error:
-        kernel = 'star_kernel<double,H=3>'
+        kernel = f'star_kernel<{cname},H=3>'
     nat.check(nat.lib().gb_set_stencil_path(args.stencil_path), 'stencil path')
     if args.stencil_path == 1:
-        kernel = 'star_kernel<double,H=3>'
+        kernel = f'star_kernel<{cname},H=3>'
 
     for _ in range(max(args.warmup, 3)):
         lap.apply(x, y)
@@ -495,7 +503,7 @@ def main():
     if args.kernel_only:
         if rank == 0:
             print(json.dumps({'metric': METRIC, 'value': round(value, 1), 'unit': 'GB/s',
-                              'bands': nb, 'kernel': kernel,
+                              'bands': nb, 'dtype': args.dtype, 'kernel': kernel,
                               'ms_per_step': round(total_ms / args.steps, 4),
                               'launch_ms': round(launch_ms, 4), 'clocks': clk}))
         if world > 1:

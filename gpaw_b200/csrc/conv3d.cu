@@ -12,10 +12,12 @@
 // Activations are FP32, weights BF16 (converted to FP32 in shared memory),
 // accumulation FP32.  Boundaries per axis: zero padding or periodic wrap
 // (the grid's own boundary conditions).  Forward: a CTA covers 1 x 16 x 32
-// points; input channels are staged with their halo in shared memory four
-// at a time, the weights once, laid out [ci][k][co] so that four output
+// points (1 x 32 x 32 for one output channel); input channels are staged
+// with their halo in shared memory four at a time (a warp per row, lanes
+// over columns), the weights once, laid out [ci][k][co] so that four output
 // channels' weights come in one 16-byte broadcast load; every thread keeps
-// 4 consecutive points x all output channels in registers.  Backward-weight: CTAs
+// 4 (8 for one output channel) consecutive points x all output channels in
+// registers.  Backward-weight: CTAs
 // over (co, ci) pairs x chunks of the points; each reduces its chunk's 27
 // sums and adds them to dw with FP32 atomics (dw accumulates, as before).
 #include <cuda_bf16.h>
@@ -36,11 +38,15 @@ struct ConvArgs {
 };
 
 // forward tile: one plane (axis 0) x CY rows x CZ points; a thread owns PX
-// consecutive points of one row and all COUT outputs of them
-constexpr int CY = 16, CZ = 32, PX = 4;
-constexpr int CTHREADS = CY * (CZ / PX);            // 128
-constexpr int SY = CY + 2, SZP = 36;                 // staged rows, padded row pitch (floats)
-constexpr int CCH = 4;                               // input channels staged per pass
+// consecutive points of one row and all COUT outputs of them.  Single-output
+// convolutions use PX = 8 (one weight load per 8 FMAs), the others PX = 4.
+constexpr int CZ = 32, CTHREADS = 128, CCH = 4;
+template <int COUT> struct ConvTile {
+  static constexpr int PX = COUT == 1 ? 8 : 4;
+  static constexpr int CY = CTHREADS / (CZ / PX);      // 32 or 16 rows
+  static constexpr int SY = CY + 2;                    // staged rows
+  static constexpr int SZP = CZ + PX;                  // padded row pitch (floats), >= CZ + 2, multiple of 4
+};
 
 __device__ __forceinline__ int cwrap(int i, int n) {
   int r = i % n;
@@ -49,11 +55,13 @@ __device__ __forceinline__ int cwrap(int i, int n) {
 
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(CTHREADS) conv3d_fwd_kernel(const ConvArgs a) {
+  using TL = ConvTile<COUT>;
+  constexpr int PX = TL::PX, CY = TL::CY, SY = TL::SY, SZP = TL::SZP;
   constexpr int CC = CIN < CCH ? CIN : CCH;
   extern __shared__ __align__(16) float conv_smem[];
-  float* sw = conv_smem;                               // [ci][k][co]
+  float* sw = conv_smem;                                     // [ci][k][co]
   float* sx = conv_smem + ((CIN * 27 * COUT + 3) / 4) * 4;   // [cc][3][SY][SZP]
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int e = tid; e < COUT * CIN * 27; e += CTHREADS) {
     const int co = e / (CIN * 27), ci = (e / 27) % CIN, k = e % 27;
     sw[(ci * 27 + k) * COUT + co] = __bfloat162float(a.w[e]);
@@ -68,6 +76,11 @@ __global__ void __launch_bounds__(CTHREADS) conv3d_fwd_kernel(const ConvArgs a) 
     const int i0 = (int)(r / (tyn * tzn));
     r %= tyn * tzn;
     const int j0 = (int)(r / tzn) * CY, k0 = (int)(r % tzn) * CZ;
+    // the staged columns of this lane (fixed for the tile)
+    int gz0 = k0 - 1 + lane, gz1 = k0 - 1 + 32 + lane;
+    bool oz0 = true, oz1 = lane < 2;
+    if (gz0 < 0 || gz0 >= a.n2) { if (a.pbc2) gz0 = cwrap(gz0, a.n2); else oz0 = false; }
+    if (gz1 < 0 || gz1 >= a.n2) { if (a.pbc2) gz1 = cwrap(gz1, a.n2); else oz1 = false; }
     float acc[PX][COUT];
 #pragma unroll
     for (int p = 0; p < PX; ++p)
@@ -75,17 +88,23 @@ __global__ void __launch_bounds__(CTHREADS) conv3d_fwd_kernel(const ConvArgs a) 
       for (int co = 0; co < COUT; ++co) acc[p][co] = 0.f;
     for (int c0 = 0; c0 < CIN; c0 += CC) {
       __syncthreads();   // previous pass (and the weight staging) done
-      for (int e = tid; e < CC * 3 * SY * (CZ + 2); e += CTHREADS) {
-        const int kk = e % (CZ + 2), jj = (e / (CZ + 2)) % SY, ii = (e / ((CZ + 2) * SY)) % 3;
-        const int cc = e / ((CZ + 2) * SY * 3);
-        int g0 = i0 - 1 + ii, g1 = j0 - 1 + jj, g2 = k0 - 1 + kk;
+      // one warp per staged row (channel, plane, row): lanes over columns
+      for (int row = warp; row < CC * 3 * SY; row += CTHREADS / 32) {
+        const int jj = row % SY, ii = (row / SY) % 3, cc = row / (3 * SY);
+        int g0 = i0 - 1 + ii, g1 = j0 - 1 + jj;
         bool ok = true;
         if (g0 < 0 || g0 >= a.n0) { if (a.pbc0) g0 = cwrap(g0, a.n0); else ok = false; }
         if (g1 < 0 || g1 >= a.n1) { if (a.pbc1) g1 = cwrap(g1, a.n1); else ok = false; }
-        if (g2 < 0 || g2 >= a.n2) { if (a.pbc2) g2 = cwrap(g2, a.n2); else ok = false; }
-        sx[((cc * 3 + ii) * SY + jj) * SZP + kk] =
-            ok ? a.x[(b * CIN + c0 + cc) * n012 + ((int64_t)g0 * a.n1 + g1) * a.n2 + g2] : 0.f;
+        const float* src = a.x + (b * CIN + c0 + cc) * n012 + ((int64_t)g0 * a.n1 + g1) * a.n2;
+        float* dst = sx + row * SZP;
+        // asynchronous 4-byte copies: every row's loads are in flight at once
+        if (ok && oz0) cp_async4(dst + lane, src + gz0); else dst[lane] = 0.f;
+        if (lane < 2) {
+          if (ok && oz1) cp_async4(dst + 32 + lane, src + gz1); else dst[32 + lane] = 0.f;
+        }
       }
+      cp_async_commit();
+      cp_async_wait<0>();
       __syncthreads();
 #pragma unroll 1
       for (int cc = 0; cc < CC; ++cc) {
@@ -94,11 +113,15 @@ __global__ void __launch_bounds__(CTHREADS) conv3d_fwd_kernel(const ConvArgs a) 
         for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
           for (int dy = 0; dy < 3; ++dy) {
-            const float* row = sx + ((cc * 3 + dx) * SY + ty + dy) * SZP + tz;
+            const float* rowp = sx + ((cc * 3 + dx) * SY + ty + dy) * SZP + tz;
             float in[PX + 2];
-            const float4 v4 = *reinterpret_cast<const float4*>(row);
-            in[0] = v4.x; in[1] = v4.y; in[2] = v4.z; in[3] = v4.w;
-            in[4] = row[4]; in[5] = row[5];
+#pragma unroll
+            for (int q = 0; q < PX; q += 4) {
+              const float4 v4 = *reinterpret_cast<const float4*>(rowp + q);
+              in[q] = v4.x; in[q + 1] = v4.y; in[q + 2] = v4.z; in[q + 3] = v4.w;
+            }
+            in[PX] = rowp[PX];
+            in[PX + 1] = rowp[PX + 1];
 #pragma unroll
             for (int dz = 0; dz < 3; ++dz) {
               const float* wk = wc + (dx * 9 + dy * 3 + dz) * COUT;
@@ -189,9 +212,10 @@ __global__ void __launch_bounds__(256) conv3d_bwd_w_kernel(const float* __restri
 
 template <int CIN, int COUT>
 static int fwd_launch(const ConvArgs& a, cudaStream_t st) {
+  using TL = ConvTile<COUT>;
   constexpr int CC = CIN < CCH ? CIN : CCH;
-  const int64_t tiles = (int64_t)a.n0 * ((a.n1 + CY - 1) / CY) * ((a.n2 + CZ - 1) / CZ) * a.nb;
-  const size_t smem = (size_t)(((CIN * 27 * COUT + 3) / 4) * 4 + CC * 3 * SY * SZP) * sizeof(float);
+  const int64_t tiles = (int64_t)a.n0 * ((a.n1 + TL::CY - 1) / TL::CY) * ((a.n2 + CZ - 1) / CZ) * a.nb;
+  const size_t smem = (size_t)(((CIN * 27 * COUT + 3) / 4) * 4 + CC * 3 * TL::SY * TL::SZP) * sizeof(float);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(conv3d_fwd_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -19,6 +19,11 @@
 // (tma.cuh).
 #include <algorithm>
 #include <cstring>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
 #include <cudaTypedefs.h>
 #include "internal.cuh"
 #include "tma.cuh"
@@ -59,6 +64,19 @@ bool encode_tensor_map_4d(CUtensorMap* map, CUtensorMapDataType dt, void* base, 
 }
 
 static thread_local const char* g_tma_reason = "";
+// autotuner state: layout key -> chosen rows-per-thread-row count (ty)
+static std::mutex g_tune_mutex;
+static std::map<std::string, int> g_tune;
+// GPAW_B200_AUTOTUNE=0 turns timing off (the model's choice is launched):
+// makes the launch sequence of a run reproducible, e.g. for a profiler
+static int autotune_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("GPAW_B200_AUTOTUNE");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v;
+}
 constexpr int NS_MAX = 16;      // ring slots (mbarrier pairs live in the first 256 bytes)
 
 struct TmaArgs {
@@ -69,6 +87,7 @@ struct TmaArgs {
   int n0, n1, n2;
   int pbc0, pbc1, pbc2;
   int TY, TZ, NTC, T1, ROWS, ytiles, NS;
+  int T1L;          // rows of the last row tile of a periodic axis 1 (<= T1)
   int pitch;        // bytes per shared-memory row (multiple of 128, >= n2 * sizeof(T))
   int slot_bytes;   // ROWS * pitch
   double c0;
@@ -113,6 +132,7 @@ template <typename T, int H, int R1, int R2, int VB>
 __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                         const __grid_constant__ CUtensorMap tmH,
                                                         const __grid_constant__ CUtensorMap tmB,
+                                                        const __grid_constant__ CUtensorMap tmL,
                                                         const __grid_constant__ TmaArgs a) {
   using R = typename Elem<T>::R;
   constexpr int VEC = VB / (int)sizeof(T);   // elements per vector access
@@ -151,6 +171,7 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
       tma_prefetch_desc(&tmA);
       tma_prefetch_desc(&tmH);
       tma_prefetch_desc(&tmB);
+      tma_prefetch_desc(&tmL);
       const int tile_kind_first = a.pbc1 ? 1 : 0;
       // ring position and the parity of the empty barrier to wait on (no wait
       // during the first pass over the ring)
@@ -166,7 +187,9 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
         const int band = (int)(col / a.ytiles);
         const int y0 = (int)(col % a.ytiles) * T1;
         // 0: one box; 1: first tile of a periodic axis 1; 2: last tile of it
-        const int kind = (tile_kind_first && y0 == 0) ? 1 : (a.pbc1 && y0 + T1 == n1) ? 2 : 0;
+        const int kind = (tile_kind_first && y0 == 0) ? 1 : (a.pbc1 && y0 + T1 >= n1) ? 2 : 0;
+        // the last tile of a periodic axis 1 may be shorter (T1L rows)
+        const uint32_t bytes = kind == 2 ? (uint32_t)((a.T1L + 2 * H) * a.pitch) : (uint32_t)a.slot_bytes;
         const int L = p_end - p_start + 2 * H;
         for (int t = 0; t < L; ++t) {
           if (!first_pass && !mbar_wait(&empty[slot], eph)) {
@@ -178,15 +201,15 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
           // and n0..n0+H-1 as TMA out-of-bounds fill (zeros)
           if (a.pbc0) sp = sp < 0 ? sp + n0 : (sp >= n0 ? sp - n0 : sp);
           unsigned char* dst = slots + (int64_t)slot * a.slot_bytes;
-          mbar_arrive_expect_tx(&full[slot], (uint32_t)a.slot_bytes);
+          mbar_arrive_expect_tx(&full[slot], bytes);
           if (kind == 0) {
             tma_load_4d(dst, &tmA, &full[slot], 0, y0 - H, sp, band);
           } else if (kind == 1) {
             tma_load_4d(dst, &tmH, &full[slot], 0, n1 - H, sp, band);
             tma_load_4d(dst + H * a.pitch, &tmB, &full[slot], 0, 0, sp, band);
           } else {
-            tma_load_4d(dst, &tmB, &full[slot], 0, y0 - H, sp, band);
-            tma_load_4d(dst + (T1 + H) * a.pitch, &tmH, &full[slot], 0, 0, sp, band);
+            tma_load_4d(dst, &tmL, &full[slot], 0, y0 - H, sp, band);
+            tma_load_4d(dst + (a.T1L + H) * a.pitch, &tmH, &full[slot], 0, 0, sp, band);
           }
           if (++slot == NS) {
             slot = 0;
@@ -409,7 +432,8 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
   for (int ty = 1; ty * TZ <= 512 - 32 && ncand < 250; ++ty) {
     const int T1 = ty * R1;
     if (T1 < H || T1 + 2 * H > 256) continue;
-    if (op->pbc[1] && (n1 % T1 != 0 || n1 / T1 < 2)) continue;
+    // periodic axis 1: at least two tiles, the last one at least H rows
+    if (op->pbc[1] && (ceil_div(n1, T1) < 2 || n1 - (ceil_div(n1, T1) - 1) * T1 < H)) continue;
     if (!op->pbc[1] && T1 > n1 + R1 - 1) continue;
     const int threads = ((ty * TZ + 31) / 32) * 32 + 32;
     const int regs_cta = threads * ((regs + 7) / 8 * 8);
@@ -420,74 +444,149 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
       const int ns = std::min(NS_MAX, per_cta / slot);
       if (ns < H + 3) continue;
       const double cw = std::min(24.0, ctas * ((ty * TZ + 31) / 32.0));
-      const double eff = (double)T1 / (T1 + 2.0 * H);
+      // useful rows per staged row: halo rows and the empty part of a short
+      // last tile both count against a tile height
+      const double eff = (double)n1 / ((double)ceil_div(n1, T1) * (T1 + 2.0 * H));
       const double pf = std::min(1.0, (ns - H - 1) / 4.0);
       cands[ncand++] = {cw * eff * pf, ty, ctas, ns};
     }
   }
   std::sort(cands, cands + ncand, [](const Cand& x, const Cand& y) { return x.score > y.score; });
-  int best = -1, occ = 0;
-  for (int c = 0; c < ncand && best < 0; ++c) {
-    const int th = ((cands[c].ty * TZ + 31) / 32) * 32 + 32;
-    const size_t sm = 256 + 128 + (size_t)cands[c].ns * (cands[c].ty * R1 + 2 * H) * pitch;
+  // the occupancy-checked candidates kept for tuning (distinct row-tile
+  // heights): the model's best three, the best tile height that divides n1
+  // (no short last tile), and the best configuration with several CTAs per SM
+  constexpr int NOK = 6;
+  Cand ok[NOK];
+  int occ_of[NOK];
+  int nok = 0;
+  auto try_add = [&](const Cand& cd) -> bool {
+    for (int i = 0; i < nok; ++i)
+      if (ok[i].ty == cd.ty) return false;
+    const int th = ((cd.ty * TZ + 31) / 32) * 32 + 32;
+    const size_t sm = 256 + 128 + (size_t)cd.ns * (cd.ty * R1 + 2 * H) * pitch;
     int o = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, th, sm) == cudaSuccess && o >= cands[c].ctas) {
-      best = c;
-      occ = o;
+    if (nok < NOK && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, th, sm) == cudaSuccess &&
+        o >= cd.ctas) {
+      ok[nok] = cd;
+      occ_of[nok++] = o;
+      return true;
+    }
+    return false;
+  };
+  for (int c = 0; c < ncand && nok < 3; ++c) try_add(cands[c]);
+  for (int c = 0; c < ncand; ++c)
+    if (n1 % (cands[c].ty * R1) == 0 && try_add(cands[c])) break;
+  for (int c = 0; c < ncand; ++c)
+    if (cands[c].ctas > 1 && try_add(cands[c])) break;
+  cudaGetLastError();
+  if (nok == 0) {
+    g_tma_reason = ncand ? "zero occupancy" : "no row tile fits the grid";
+    return 1;
+  }
+
+  // one launch of candidate c
+  auto launch = [&](int c) -> int {
+    const Cand cb = ok[c];
+    TmaArgs a{};
+    a.out = out; a.y = ep.y; a.vpot = ep.vpot; a.nbatch = nin;
+    a.n0 = n0; a.n1 = n1; a.n2 = n2;
+    a.pbc0 = op->pbc[0]; a.pbc1 = op->pbc[1]; a.pbc2 = op->pbc[2];
+    a.TY = cb.ty; a.TZ = TZ; a.NTC = cb.ty * TZ; a.T1 = cb.ty * R1; a.ROWS = a.T1 + 2 * H;
+    a.ytiles = ceil_div(n1, a.T1);
+    a.T1L = n1 - (a.ytiles - 1) * a.T1;
+    a.NS = cb.ns;
+    a.pitch = pitch;
+    a.slot_bytes = a.ROWS * pitch;
+    a.c0 = op->center;
+    a.c0diff = op->center;
+    for (int cc = 0; cc < 3; ++cc)
+      for (int m = 0; m < 2 * HMAX + 1; ++m) a.c0diff += op->a[cc][m];
+    memcpy(a.a, op->a, sizeof(a.a));
+    a.c0f = (float)a.c0;
+    a.c0difff = (float)a.c0diff;
+    for (int cc = 0; cc < 3; ++cc)
+      for (int m = 0; m < 2 * HMAX + 1; ++m) a.af[cc][m] = (float)op->a[cc][m];
+    a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma;
+    const size_t smem = 256 + 128 + (size_t)a.NS * a.slot_bytes;
+    // tensor maps over (n2 scalars, n1, n0, nbatch); the box spans the whole
+    // padded pitch, so the columns past n2 arrive as zeros
+    const int scal = Elem<T>::cplx ? 2 : 1;
+    const CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const uint64_t es = sizeof(R);
+    const uint64_t dims[4] = {(uint64_t)n2 * scal, (uint64_t)n1, (uint64_t)n0, (uint64_t)nin};
+    const uint64_t strides[3] = {dims[0] * es, dims[0] * dims[1] * es, dims[0] * dims[1] * dims[2] * es};
+    const uint32_t bx = (uint32_t)(pitch / (int)es);
+    CUtensorMap tmA, tmH, tmB, tmL;
+    const uint32_t boxA[4] = {bx, (uint32_t)a.ROWS, 1, 1};
+    const uint32_t boxH[4] = {bx, (uint32_t)H, 1, 1};
+    const uint32_t boxB[4] = {bx, (uint32_t)(a.T1 + H), 1, 1};
+    const uint32_t boxL[4] = {bx, (uint32_t)(a.T1L + H), 1, 1};
+    void* base = const_cast<void*>(in);
+    if (!encode_tensor_map_4d(&tmA, dt, base, dims, strides, boxA) ||
+        !encode_tensor_map_4d(&tmH, dt, base, dims, strides, boxH) ||
+        !encode_tensor_map_4d(&tmB, dt, base, dims, strides, boxB) ||
+        !encode_tensor_map_4d(&tmL, dt, base, dims, strides, boxL)) {
+      g_tma_reason = "cuTensorMapEncodeTiled rejected the layout";
+      return 1;
+    }
+    const int threads = ((a.NTC + 31) / 32) * 32 + 32;
+    const int64_t total = nin * (int64_t)a.ytiles * n0;
+    int64_t blocks = (int64_t)sm_count() * std::min(occ_of[c], cb.ctas);
+    blocks = std::min<int64_t>(blocks, std::max<int64_t>(1, total / (4 * H + 4)));
+    kern<<<(unsigned)blocks, threads, smem, st>>>(tmA, tmH, tmB, tmL, a);
+    return check_launch("star_tma_kernel");
+  };
+
+  // autotuning: the first call for a layout (grid, boundaries, dtype, radius,
+  // epilogue kind, batch) times the candidates with CUDA events on its own
+  // data -- every launch writes the same output, so the call stays exact --
+  // and later calls launch the winner.  Inside a stream capture, or if timing
+  // fails, the model's best candidate is used without tuning.
+  const int epi_kind = (ep.vpot ? 4 : 0) | (ep.y ? 2 : 0) | ((ep.alpha != 1.0 || ep.beta != 0.0) ? 1 : 0);
+  char keyb[160];
+  snprintf(keyb, sizeof keyb, "%d:%d:%d:%d:%d:%d:%d:%d:%d:%d:%lld", (int)sizeof(T), Elem<T>::cplx ? 1 : 0, H, n0, n1,
+           n2, op->pbc[0] * 4 + op->pbc[1] * 2 + op->pbc[2], epi_kind, (int)VB, R2, (long long)nin);
+  const std::string key(keyb);
+  int choice = -1;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto f = g_tune.find(key);
+    if (f != g_tune.end())
+      for (int c = 0; c < nok; ++c)
+        if (ok[c].ty == f->second) choice = c;
+  }
+  if (choice < 0 && nok > 1 && autotune_enabled()) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusNone) {
+      cudaEvent_t e0, e1;
+      if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+        float best_ms = 1e30f;
+        for (int c = 0; c < nok; ++c) {
+          if (launch(c)) continue;   // warm-up run of this shape
+          cudaEventRecord(e0, st);
+          int bad = 0;
+          for (int r = 0; r < 2; ++r) bad |= launch(c);
+          cudaEventRecord(e1, st);
+          float ms = 0.f;
+          if (!bad && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
+              ms < best_ms) {
+            best_ms = ms;
+            choice = c;
+          }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+      }
+      cudaGetLastError();
+      if (choice >= 0) {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune[key] = ok[choice].ty;
+      }
     }
   }
-  cudaGetLastError();
-  if (best < 0) {
-    g_tma_reason = ncand ? "zero occupancy" : "no row tile fits the grid (periodic axis 1 needs T1 | n1)";
-    return 1;
-  }
-  const Cand cb = cands[best];
-  TmaArgs a{};
-  a.out = out; a.y = ep.y; a.vpot = ep.vpot; a.nbatch = nin;
-  a.n0 = n0; a.n1 = n1; a.n2 = n2;
-  a.pbc0 = op->pbc[0]; a.pbc1 = op->pbc[1]; a.pbc2 = op->pbc[2];
-  a.TY = cb.ty; a.TZ = TZ; a.NTC = cb.ty * TZ; a.T1 = cb.ty * R1; a.ROWS = a.T1 + 2 * H;
-  a.ytiles = ceil_div(n1, a.T1);
-  a.NS = cb.ns;
-  a.pitch = pitch;
-  a.slot_bytes = a.ROWS * pitch;
-  a.c0 = op->center;
-  a.c0diff = op->center;
-  for (int c = 0; c < 3; ++c)
-    for (int m = 0; m < 2 * HMAX + 1; ++m) a.c0diff += op->a[c][m];
-  memcpy(a.a, op->a, sizeof(a.a));
-  a.c0f = (float)a.c0;
-  a.c0difff = (float)a.c0diff;
-  for (int c = 0; c < 3; ++c)
-    for (int m = 0; m < 2 * HMAX + 1; ++m) a.af[c][m] = (float)op->a[c][m];
-  a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma;
-  const size_t smem = 256 + 128 + (size_t)a.NS * a.slot_bytes;
-  // tensor maps over (n2 scalars, n1, n0, nbatch); the box spans the whole
-  // padded pitch, so the columns past n2 arrive as zeros
-  const int scal = Elem<T>::cplx ? 2 : 1;
-  const CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-  const uint64_t es = sizeof(R);
-  const uint64_t dims[4] = {(uint64_t)n2 * scal, (uint64_t)n1, (uint64_t)n0, (uint64_t)nin};
-  const uint64_t strides[3] = {dims[0] * es, dims[0] * dims[1] * es, dims[0] * dims[1] * dims[2] * es};
-  const uint32_t bx = (uint32_t)(pitch / (int)es);
-  CUtensorMap tmA, tmH, tmB;
-  const uint32_t boxA[4] = {bx, (uint32_t)a.ROWS, 1, 1};
-  const uint32_t boxH[4] = {bx, (uint32_t)H, 1, 1};
-  const uint32_t boxB[4] = {bx, (uint32_t)(a.T1 + H), 1, 1};
-  void* base = const_cast<void*>(in);
-  if (!encode_tensor_map_4d(&tmA, dt, base, dims, strides, boxA) ||
-      !encode_tensor_map_4d(&tmH, dt, base, dims, strides, boxH) ||
-      !encode_tensor_map_4d(&tmB, dt, base, dims, strides, boxB)) {
-    g_tma_reason = "cuTensorMapEncodeTiled rejected the layout";
-    return 1;
-  }
-  const int threads = ((a.NTC + 31) / 32) * 32 + 32;
-  const int64_t total = nin * (int64_t)a.ytiles * n0;
-  int64_t blocks = (int64_t)sm_count() * std::min(occ, cb.ctas);
-  blocks = std::min<int64_t>(blocks, std::max<int64_t>(1, total / (4 * H + 4)));
-  kern<<<(unsigned)blocks, threads, smem, st>>>(tmA, tmH, tmB, a);
-  const int rc = check_launch("star_tma_kernel");
-  return rc;
+  if (choice < 0) choice = 0;
+  return launch(choice);
 }
 
 static int g_stencil_path = 0;   // 0 auto, 1 cp.async only, 2 TMA required
