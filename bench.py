@@ -342,6 +342,41 @@ def scf_benchmark(train_steps=400):
     return out
 
 
+def network_benchmark(args):
+    """The learned preconditioner's forward pass on its production shape:
+    160 FP32 residuals of the 56^3 periodic Si64 grid (h = 0.194 A), the
+    network initialised from the V-cycle; CUDA events around `steps` passes
+    after `warmup` untimed ones, next to the fused V-cycle on the same data."""
+    import torch
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.fd_operators import Laplace
+    from gpaw_b200.preconditioner import Preconditioner
+    from gpaw_b200.learned import ConvNet
+    cell = 10.86 / BOHR
+    gd = GridDescriptor((56, 56, 56), (cell, cell, cell), True)
+    mg = Preconditioner(gd, Laplace(gd, -0.5, 3), float)
+    net = ConvNet(gd).init_from_multigrid(mg)
+    g = torch.Generator(device='cuda').manual_seed(0)
+    R = torch.randn((160, 56, 56, 56), generator=g, device='cuda', dtype=torch.float32)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+    out = {'workload': 'learned preconditioner forward, 160 x 56^3 FP32 residuals',
+           'network_ms': round(timed(lambda: net.forward(R)), 4),
+           'vcycle_ms': round(timed(lambda: mg(R)), 4)}
+    print(json.dumps(out))
+
+
 def cpu_reference_rate(nb_sample, threads, reps=3):
     """GPAW's own C Operator (oracle/_ref) on the host: best-of GB/s."""
     from oracle import ref, fd
@@ -422,6 +457,10 @@ def main():
     ap.add_argument('--kernel-only', action='store_true',
                     help='time the stencil step only (no e2e, suite or CPU '
                          'baseline): the command line used for ncu captures')
+    ap.add_argument('--network-only', action='store_true',
+                    help='time the learned preconditioner network alone: one '
+                         'forward pass over 160 FP32 residuals of the 56^3 Si64 '
+                         'grid per step (the command line used for ncu captures)')
     ap.add_argument('--dtype', default='f64', choices=['f64', 'f32'],
                     help='storage precision of the kernel-only run (the '
                          'benchmark line itself is FP64)')
@@ -431,6 +470,9 @@ def main():
     if args.impl == 'reference':
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count() or 1))
         run_reference(args)
+        return
+    if args.network_only:
+        network_benchmark(args)
         return
 
     import torch
