@@ -48,6 +48,9 @@ _SIGNATURES = {
                                    c_int, POINTER(c_void_p)]),
     'gb_transformer_apply': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,
                                      c_int, PD, c_void_p]),
+    'gb_transformer_apply_axpy': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,
+                                          c_int, PD, c_double, c_void_p, c_double,
+                                          c_void_p]),
     'gb_transformer_free': (c_int, [c_void_p]),
     'gb_fd_precond_noalloc': (c_int, [c_void_p] * 7 + [c_void_p, c_void_p,
                                                         c_double, c_int64, c_int,
@@ -64,6 +67,8 @@ _SIGNATURES = {
                                   c_void_p, c_void_p]),
     'gb_conv3d_forward': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int,
                                   c_int, P64, POINTER(c_int), c_int, c_void_p]),
+    'gb_conv3d_forward_pair': (c_int, [c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_int64, P64, POINTER(c_int), c_void_p]),
     'gb_conv3d_backward_weight': (c_int, [c_void_p, c_void_p, c_void_p, c_int64,
                                           c_int, c_int, P64, POINTER(c_int),
                                           c_void_p]),

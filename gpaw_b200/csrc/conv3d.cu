@@ -28,6 +28,7 @@ namespace gb {
 
 struct ConvArgs {
   const float* x;
+  const float* x2;          // when set: input channel 1 comes from here (CIN = 2)
   float* y;
   const __nv_bfloat16* w;   // [cout][cin][27]
   int64_t nb;
@@ -37,15 +38,23 @@ struct ConvArgs {
   int accumulate;           // y += conv(x) instead of y = conv(x)
 };
 
-// forward tile: one plane (axis 0) x CY rows x CZ points; a thread owns PX
-// consecutive points of one row and all COUT outputs of them.  Single-output
-// convolutions use PX = 8 (one weight load per 8 FMAs), the others PX = 4.
-constexpr int CZ = 32, CTHREADS = 128, CCH = 4;
-template <int COUT> struct ConvTile {
+// forward tile: one plane (axis 0) x CY rows x CZT points; a thread owns PX
+// consecutive points of one row and all COUT outputs of them (PX = 8 for a
+// single output channel: one weight load per 8 FMAs; 4 otherwise).  Rows of
+// at most 16 points use 16-wide tiles.  The shared row pitch keeps the
+// 16-byte loads of a warp free of bank conflicts on 32-wide tiles (2-way on
+// 16-wide ones).
+constexpr int CCH = 4;
+template <int COUT, int CZT> struct ConvTile {
   static constexpr int PX = COUT == 1 ? 8 : 4;
-  static constexpr int CY = CTHREADS / (CZ / PX);      // 32 or 16 rows
-  static constexpr int SY = CY + 2;                    // staged rows
-  static constexpr int SZP = CZ + PX;                  // padded row pitch (floats), >= CZ + 2, multiple of 4
+  static constexpr int CY = 16 * (CZT == 32 && COUT == 1 ? 2 : 1);
+  static constexpr int THREADS = CY * (CZT / PX);
+  static constexpr int SY = CY + 2;
+  // staged window: global columns k0 - 4 .. k0 + CZT + 3 (16-byte chunks when
+  // the row length is a multiple of 4); pitch free of bank conflicts for the
+  // 16-byte loads on 32-wide tiles
+  static constexpr int CH = (CZT + 8) / 4;           // chunks per staged row
+  static constexpr int SZP = CZT == 32 ? (PX == 8 ? 44 : 40) : CZT + 12;
 };
 
 __device__ __forceinline__ int cwrap(int i, int n) {
@@ -53,34 +62,33 @@ __device__ __forceinline__ int cwrap(int i, int n) {
   return r < 0 ? r + n : r;
 }
 
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(CTHREADS) conv3d_fwd_kernel(const ConvArgs a) {
-  using TL = ConvTile<COUT>;
-  constexpr int PX = TL::PX, CY = TL::CY, SY = TL::SY, SZP = TL::SZP;
+template <int CIN, int COUT, int CZT>
+__global__ void __launch_bounds__(ConvTile<COUT, CZT>::THREADS) conv3d_fwd_kernel(const ConvArgs a) {
+  using TL = ConvTile<COUT, CZT>;
+  constexpr int PX = TL::PX, CY = TL::CY, SY = TL::SY, SZP = TL::SZP, NT = TL::THREADS;
   constexpr int CC = CIN < CCH ? CIN : CCH;
+  constexpr int NW = (NT + 31) / 32;
   extern __shared__ __align__(16) float conv_smem[];
   float* sw = conv_smem;                                     // [ci][k][co]
   float* sx = conv_smem + ((CIN * 27 * COUT + 3) / 4) * 4;   // [cc][3][SY][SZP]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int e = tid; e < COUT * CIN * 27; e += CTHREADS) {
+  for (int e = tid; e < COUT * CIN * 27; e += NT) {
     const int co = e / (CIN * 27), ci = (e / 27) % CIN, k = e % 27;
     sw[(ci * 27 + k) * COUT + co] = __bfloat162float(a.w[e]);
   }
-  const int tyn = (a.n1 + CY - 1) / CY, tzn = (a.n2 + CZ - 1) / CZ;
+  const int tyn = (a.n1 + CY - 1) / CY, tzn = (a.n2 + CZT - 1) / CZT;
   const int64_t ntile = (int64_t)a.n0 * tyn * tzn;
   const int64_t n012 = (int64_t)a.n0 * a.n1 * a.n2;
-  const int ty = tid / (CZ / PX), tz = (tid % (CZ / PX)) * PX;
+  const int ty = tid / (CZT / PX), tz = (tid % (CZT / PX)) * PX;
+  const int xin = a.x2 ? 1 : CIN;     // channels per sample in x
+  const bool vec_rows = (a.n2 % 4) == 0;   // 16-byte aligned rows: chunk staging
+  const bool even_rows = (a.n2 % 2) == 0;  // 8-byte aligned rows
   for (int64_t t = blockIdx.x; t < ntile * a.nb; t += gridDim.x) {
     const int64_t b = t / ntile;
     int64_t r = t % ntile;
     const int i0 = (int)(r / (tyn * tzn));
     r %= tyn * tzn;
-    const int j0 = (int)(r / tzn) * CY, k0 = (int)(r % tzn) * CZ;
-    // the staged columns of this lane (fixed for the tile)
-    int gz0 = k0 - 1 + lane, gz1 = k0 - 1 + 32 + lane;
-    bool oz0 = true, oz1 = lane < 2;
-    if (gz0 < 0 || gz0 >= a.n2) { if (a.pbc2) gz0 = cwrap(gz0, a.n2); else oz0 = false; }
-    if (gz1 < 0 || gz1 >= a.n2) { if (a.pbc2) gz1 = cwrap(gz1, a.n2); else oz1 = false; }
+    const int j0 = (int)(r / tzn) * CY, k0 = (int)(r % tzn) * CZT;
     float acc[PX][COUT];
 #pragma unroll
     for (int p = 0; p < PX; ++p)
@@ -88,19 +96,72 @@ __global__ void __launch_bounds__(CTHREADS) conv3d_fwd_kernel(const ConvArgs a) 
       for (int co = 0; co < COUT; ++co) acc[p][co] = 0.f;
     for (int c0 = 0; c0 < CIN; c0 += CC) {
       __syncthreads();   // previous pass (and the weight staging) done
-      // one warp per staged row (channel, plane, row): lanes over columns
-      for (int row = warp; row < CC * 3 * SY; row += CTHREADS / 32) {
-        const int jj = row % SY, ii = (row / SY) % 3, cc = row / (3 * SY);
-        int g0 = i0 - 1 + ii, g1 = j0 - 1 + jj;
-        bool ok = true;
-        if (g0 < 0 || g0 >= a.n0) { if (a.pbc0) g0 = cwrap(g0, a.n0); else ok = false; }
-        if (g1 < 0 || g1 >= a.n1) { if (a.pbc1) g1 = cwrap(g1, a.n1); else ok = false; }
-        const float* src = a.x + (b * CIN + c0 + cc) * n012 + ((int64_t)g0 * a.n1 + g1) * a.n2;
-        float* dst = sx + row * SZP;
-        // asynchronous 4-byte copies: every row's loads are in flight at once
-        if (ok && oz0) cp_async4(dst + lane, src + gz0); else dst[lane] = 0.f;
-        if (lane < 2) {
-          if (ok && oz1) cp_async4(dst + 32 + lane, src + gz1); else dst[32 + lane] = 0.f;
+      if (vec_rows) {
+        // 16-byte chunks: a warp stages 32 / CH rows per iteration
+        constexpr int RPW = 32 / TL::CH;
+        const int lr = lane / TL::CH, ck = lane % TL::CH;
+        int gz = k0 - 4 + 4 * ck;
+        bool oz = true;
+        if (gz < 0 || gz >= a.n2) { if (a.pbc2) gz = cwrap(gz, a.n2); else oz = false; }
+        for (int row0 = warp * RPW; row0 < CC * 3 * SY; row0 += NW * RPW) {
+          const int row = row0 + lr;
+          if (lr < RPW && row < CC * 3 * SY) {
+            const int jj = row % SY, ii = (row / SY) % 3, cc = row / (3 * SY);
+            int g0 = i0 - 1 + ii, g1 = j0 - 1 + jj;
+            bool ok = oz;
+            if (g0 < 0 || g0 >= a.n0) { if (a.pbc0) g0 = cwrap(g0, a.n0); else ok = false; }
+            if (g1 < 0 || g1 >= a.n1) { if (a.pbc1) g1 = cwrap(g1, a.n1); else ok = false; }
+            const int ch = c0 + cc;
+            const float* xs = (a.x2 && ch == 1) ? a.x2 : a.x;
+            const int chx = a.x2 ? 0 : ch;
+            float* dst = sx + row * SZP + 4 * ck;
+            if (ok) cp_async16(dst, xs + (b * xin + chx) * n012 + ((int64_t)g0 * a.n1 + g1) * a.n2 + gz);
+            else *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
+      } else if (even_rows) {
+        // 8-byte chunks (even row length): a warp stages 32 / CH8 rows per iteration
+        constexpr int CH8 = (CZT + 8) / 2;
+        constexpr int RPW = 32 / CH8;
+        const int lr = lane / CH8, ck = lane % CH8;
+        int gz = k0 - 4 + 2 * ck;
+        bool oz = true;
+        if (gz < 0 || gz >= a.n2) { if (a.pbc2) gz = cwrap(gz, a.n2); else oz = false; }
+        for (int row0 = warp * RPW; row0 < CC * 3 * SY; row0 += NW * RPW) {
+          const int row = row0 + lr;
+          if (lr < RPW && row < CC * 3 * SY) {
+            const int jj = row % SY, ii = (row / SY) % 3, cc = row / (3 * SY);
+            int g0 = i0 - 1 + ii, g1 = j0 - 1 + jj;
+            bool ok = oz;
+            if (g0 < 0 || g0 >= a.n0) { if (a.pbc0) g0 = cwrap(g0, a.n0); else ok = false; }
+            if (g1 < 0 || g1 >= a.n1) { if (a.pbc1) g1 = cwrap(g1, a.n1); else ok = false; }
+            const int ch = c0 + cc;
+            const float* xs = (a.x2 && ch == 1) ? a.x2 : a.x;
+            const int chx = a.x2 ? 0 : ch;
+            float* dst = sx + row * SZP + 2 * ck;
+            if (ok) cp_async8(dst, xs + (b * xin + chx) * n012 + ((int64_t)g0 * a.n1 + g1) * a.n2 + gz);
+            else *reinterpret_cast<float2*>(dst) = make_float2(0.f, 0.f);
+          }
+        }
+      } else {
+        // element copies (odd row length): one warp per row
+        for (int row = warp; row < CC * 3 * SY; row += NW) {
+          const int jj = row % SY, ii = (row / SY) % 3, cc = row / (3 * SY);
+          int g0 = i0 - 1 + ii, g1 = j0 - 1 + jj;
+          bool ok = true;
+          if (g0 < 0 || g0 >= a.n0) { if (a.pbc0) g0 = cwrap(g0, a.n0); else ok = false; }
+          if (g1 < 0 || g1 >= a.n1) { if (a.pbc1) g1 = cwrap(g1, a.n1); else ok = false; }
+          const int ch = c0 + cc;
+          const float* xs = (a.x2 && ch == 1) ? a.x2 : a.x;
+          const int chx = a.x2 ? 0 : ch;
+          const float* src = xs + (b * xin + chx) * n012 + ((int64_t)g0 * a.n1 + g1) * a.n2;
+          float* dst = sx + row * SZP;
+          for (int c = lane; c < CZT + 8; c += 32) {
+            int gz = k0 - 4 + c;
+            bool okz = ok;
+            if (gz < 0 || gz >= a.n2) { if (a.pbc2) gz = cwrap(gz, a.n2); else okz = false; }
+            if (okz) cp_async4(dst + c, src + gz); else dst[c] = 0.f;
+          }
         }
       }
       cp_async_commit();
@@ -113,15 +174,18 @@ __global__ void __launch_bounds__(CTHREADS) conv3d_fwd_kernel(const ConvArgs a) 
         for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
           for (int dy = 0; dy < 3; ++dy) {
+            // staged column c holds global column k0 - 4 + c: this thread's
+            // inputs k0 + tz - 1 .. k0 + tz + PX sit at tz + 3 .. tz + PX + 4
             const float* rowp = sx + ((cc * 3 + dx) * SY + ty + dy) * SZP + tz;
+            float win[PX + 8];
+#pragma unroll
+            for (int q = 0; q < PX + 8; q += 4) {
+              const float4 v4 = *reinterpret_cast<const float4*>(rowp + q);
+              win[q] = v4.x; win[q + 1] = v4.y; win[q + 2] = v4.z; win[q + 3] = v4.w;
+            }
             float in[PX + 2];
 #pragma unroll
-            for (int q = 0; q < PX; q += 4) {
-              const float4 v4 = *reinterpret_cast<const float4*>(rowp + q);
-              in[q] = v4.x; in[q + 1] = v4.y; in[q + 2] = v4.z; in[q + 3] = v4.w;
-            }
-            in[PX] = rowp[PX];
-            in[PX + 1] = rowp[PX + 1];
+            for (int i = 0; i < PX + 2; ++i) in[i] = win[3 + i];
 #pragma unroll
             for (int dz = 0; dz < 3; ++dz) {
               const float* wk = wc + (dx * 9 + dy * 3 + dz) * COUT;
@@ -210,22 +274,28 @@ __global__ void __launch_bounds__(256) conv3d_bwd_w_kernel(const float* __restri
   }
 }
 
+template <int CIN, int COUT, int CZT>
+static int fwd_launch_t(const ConvArgs& a, cudaStream_t st) {
+  using TL = ConvTile<COUT, CZT>;
+  constexpr int CC = CIN < CCH ? CIN : CCH;
+  const int64_t tiles = (int64_t)a.n0 * ((a.n1 + TL::CY - 1) / TL::CY) * ((a.n2 + CZT - 1) / CZT) * a.nb;
+  const size_t smem = (size_t)(((CIN * 27 * COUT + 3) / 4) * 4 + CC * 3 * TL::SY * TL::SZP) * sizeof(float);
+  auto kern = conv3d_fwd_kernel<CIN, COUT, CZT>;
+  static int per_sm = -1;
+  if (per_sm < 0) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TL::THREADS, smem);
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int64_t blocks = std::min<int64_t>(tiles, (int64_t)sm_count() * per_sm * 2);
+  kern<<<(unsigned)std::max<int64_t>(blocks, 1), TL::THREADS, smem, st>>>(a);
+  return check_launch("conv3d_fwd_kernel");
+}
+
 template <int CIN, int COUT>
 static int fwd_launch(const ConvArgs& a, cudaStream_t st) {
-  using TL = ConvTile<COUT>;
-  constexpr int CC = CIN < CCH ? CIN : CCH;
-  const int64_t tiles = (int64_t)a.n0 * ((a.n1 + TL::CY - 1) / TL::CY) * ((a.n2 + CZ - 1) / CZ) * a.nb;
-  const size_t smem = (size_t)(((CIN * 27 * COUT + 3) / 4) * 4 + CC * 3 * TL::SY * TL::SZP) * sizeof(float);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(conv3d_fwd_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3d_fwd_kernel<CIN, COUT>, CTHREADS, smem);
-  const int64_t blocks = std::min<int64_t>(tiles, (int64_t)sm_count() * std::max(per_sm, 1) * 2);
-  conv3d_fwd_kernel<CIN, COUT><<<(unsigned)std::max<int64_t>(blocks, 1), CTHREADS, smem, st>>>(a);
-  return check_launch("conv3d_fwd_kernel");
+  if (a.n2 <= 16) return fwd_launch_t<CIN, COUT, 16>(a, st);
+  return fwd_launch_t<CIN, COUT, 32>(a, st);
 }
 
 }  // namespace gb
@@ -238,7 +308,7 @@ int gb_conv3d_forward(const float* x, const void* w_bf16, float* y, int64_t nb, 
                       const int64_t n_c[3], const int pbc_c[3], int accumulate, void* stream) {
   GB_REQUIRE(x && w_bf16 && y && n_c && pbc_c && nb >= 0, "gb_conv3d_forward: bad arguments");
   if (nb == 0) return GB_OK;
-  ConvArgs a{x, y, reinterpret_cast<const __nv_bfloat16*>(w_bf16), nb, cin, cout,
+  ConvArgs a{x, nullptr, y, reinterpret_cast<const __nv_bfloat16*>(w_bf16), nb, cin, cout,
              (int)n_c[0], (int)n_c[1], (int)n_c[2], pbc_c[0], pbc_c[1], pbc_c[2], accumulate};
   cudaStream_t st = (cudaStream_t)stream;
   if (cin == 1 && cout == 1) return fwd_launch<1, 1>(a, st);
@@ -246,6 +316,15 @@ int gb_conv3d_forward(const float* x, const void* w_bf16, float* y, int64_t nb, 
   if (cin == 16 && cout == 16) return fwd_launch<16, 16>(a, st);
   if (cin == 16 && cout == 1) return fwd_launch<16, 1>(a, st);
   return fail(GB_E_UNSUPPORTED, "gb_conv3d_forward: channel pair not in {(1,1), (1,16), (16,16), (16,1)}");
+}
+
+int gb_conv3d_forward_pair(const float* x0, const float* x1, const void* w_bf16, float* y, int64_t nb,
+                           const int64_t n_c[3], const int pbc_c[3], void* stream) {
+  GB_REQUIRE(x0 && x1 && w_bf16 && y && n_c && pbc_c && nb >= 0, "gb_conv3d_forward_pair: bad arguments");
+  if (nb == 0) return GB_OK;
+  ConvArgs a{x0, x1, y, reinterpret_cast<const __nv_bfloat16*>(w_bf16), nb, 2, 1,
+             (int)n_c[0], (int)n_c[1], (int)n_c[2], pbc_c[0], pbc_c[1], pbc_c[2], 0};
+  return fwd_launch<2, 1>(a, (cudaStream_t)stream);
 }
 
 int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw, int64_t nb, int cin, int cout,

@@ -207,18 +207,31 @@ __global__ void __launch_bounds__(C::NT) restrict_kernel(const TrArgs a) {
           phase_fixup<T, FR, PITCH, PITCH, NT>(P, ry0, cx0, nf1, nf2, a, tid);
           __syncthreads();
         }
-        // pass A: along axis 2 for every staged row
-        for (int e = tid; e < FR * CZ; e += NT) {
-          const int r = e / CZ, jz = e % CZ;
-          const T* f = P + r * PITCH + sh + 2 * jz + (K - 1);
-          T x = f[0];
+        if constexpr (K == 2) {
+          // k = 2: the 3 x 3 in-plane stencil straight from the staged plane
+          // (the same operations, in the same order, as the two separable
+          // passes below; no intermediate buffer, no barrier)
+          const T* f = P + (2 * ty + 1) * PITCH + sh + 2 * tz + 1;
+          T g[3];
 #pragma unroll
-          for (int m = 0; m < K / 2; ++m) x = fmadd(x, w[m], add(f[2 * m + 1], f[-(2 * m + 1)]));
-          tbuf[r * CZ + jz] = scale(half, x);
-        }
-        __syncthreads();
-        // pass B: along axis 1 for the own coarse point
-        {
+          for (int d = 0; d < 3; ++d) {
+            const T* fr = f + (d - 1) * PITCH;
+            g[d] = scale(half, fmadd(fr[0], w[0], add(fr[1], fr[-1])));
+          }
+          u = scale(half, fmadd(g[1], w[0], add(g[2], g[0])));
+          if (CPLX) u = phase_mul(u, pr, pi);
+        } else {
+          // pass A: along axis 2 for every staged row
+          for (int e = tid; e < FR * CZ; e += NT) {
+            const int r = e / CZ, jz = e % CZ;
+            const T* f = P + r * PITCH + sh + 2 * jz + (K - 1);
+            T x = f[0];
+#pragma unroll
+            for (int m = 0; m < K / 2; ++m) x = fmadd(x, w[m], add(f[2 * m + 1], f[-(2 * m + 1)]));
+            tbuf[r * CZ + jz] = scale(half, x);
+          }
+          __syncthreads();
+          // pass B: along axis 1 for the own coarse point
           const T* tcol = tbuf + (2 * ty + (K - 1)) * CZ + tz;
           T x = tcol[0];
 #pragma unroll
@@ -242,7 +255,10 @@ __global__ void __launch_bounds__(C::NT) restrict_kernel(const TrArgs a) {
         const int yi = Y0 + ty, zi = Z0 + tz;
         if (yi < nc1 && zi < nc2) dst[(int64_t)I * nc12 + (int64_t)yi * nc2 + zi] = scale(alpha, x);
       }
-      __syncthreads();
+      // the separable passes reuse tbuf next step; the k = 2 path needs no
+      // barrier here: the slot refilled below was last read in step j - 1,
+      // which every thread finished before the barrier at the top of step j
+      if constexpr (K != 2) __syncthreads();
       if (j + D < j1) issue(j + D);
       cp_async_commit();
     }
@@ -502,10 +518,10 @@ static int launch_persistent(KernelT kernel, const TrArgs& a, int64_t total, cud
   return check_launch("transformer kernel");
 }
 
-template <typename T, int K>
-static int restrict_k(const gb_transformer* t, const void* in, void* out, int64_t nin,
-                      const double* ph, cudaStream_t st, double alpha) {
-  using C = RCfg<T, K, 8, 32, 2>;
+template <typename T, int K, int CY, int CZ>
+static int restrict_cfg(const gb_transformer* t, const void* in, void* out, int64_t nin,
+                        const double* ph, cudaStream_t st, double alpha) {
+  using C = RCfg<T, K, CY, CZ, 2>;
   TrArgs a;
   fill_common(t, a, ph);
   a.in = in; a.out = out; a.nbatch = nin; a.alpha = alpha;
@@ -513,6 +529,15 @@ static int restrict_k(const gb_transformer* t, const void* in, void* out, int64_
   a.tiles2 = ceil_div(a.no[2], C::CZ);
   const int64_t total = nin * (int64_t)a.tiles1 * a.tiles2 * a.no[0];
   return launch_persistent<C>(restrict_kernel<C>, a, total, st, 4 + K);
+}
+
+// coarse rows of at most 16 points (the coarse levels of small grids) use a
+// 16 x 16 tile, wider ones 8 x 32: no more than half a warp idles on a row
+template <typename T, int K>
+static int restrict_k(const gb_transformer* t, const void* in, void* out, int64_t nin,
+                      const double* ph, cudaStream_t st, double alpha) {
+  if (t->nout_c[2] <= 16) return restrict_cfg<T, K, 16, 16>(t, in, out, nin, ph, st, alpha);
+  return restrict_cfg<T, K, 8, 32>(t, in, out, nin, ph, st, alpha);
 }
 
 template <typename T, int K>
@@ -629,6 +654,21 @@ int gb_transformer_apply(const gb_transformer* t, const void* in, void* out, int
   GB_REQUIRE(!dtype_complex(dtype) || phase_cd, "gb_transformer_apply: complex data needs phase_cd");
   return tr_apply(t, in, out, nin, dtype, dtype_complex(dtype) ? phase_cd : nullptr,
                   (cudaStream_t)stream, 1.0, nullptr, 0.0);
+}
+
+int gb_transformer_apply_axpy(const gb_transformer* t, const void* in, void* out, int64_t nin, int dtype,
+                              const double* phase_cd, double alpha, const void* y, double gamma, void* stream) {
+  GB_REQUIRE(t, "gb_transformer_apply_axpy: null transformer");
+  GB_REQUIRE(dtype_valid(dtype), "gb_transformer_apply_axpy: unknown dtype");
+  GB_REQUIRE(nin >= 0, "gb_transformer_apply_axpy: negative batch");
+  GB_REQUIRE(dtype_complex(dtype) == !t->real,
+             "gb_transformer_apply_axpy: dtype does not match the transformer's real/complex flag");
+  if (nin == 0) return GB_OK;
+  GB_REQUIRE(in && out && in != out, "gb_transformer_apply_axpy: bad data pointers");
+  GB_REQUIRE(t->interpolate || !y, "gb_transformer_apply_axpy: restriction has no y term");
+  GB_REQUIRE(!dtype_complex(dtype) || phase_cd, "gb_transformer_apply_axpy: complex data needs phase_cd");
+  return tr_apply(t, in, out, nin, dtype, dtype_complex(dtype) ? phase_cd : nullptr, (cudaStream_t)stream, alpha,
+                  y, gamma);
 }
 
 int gb_transformer_free(gb_transformer* t) {

@@ -149,6 +149,17 @@ class ConvNet:
             nat.stream_of(x)), 'gb_conv3d_forward')
         return out
 
+    def conv_pair(self, x0, x1, w0_32, w1_32, gd):
+        """conv(x0, w0) + conv(x1, w1) for single-channel FP32 inputs, one
+        launch (gb_conv3d_forward_pair)."""
+        wb = torch.cat([w0_32, w1_32], dim=1).to(torch.bfloat16).contiguous()   # (1, 2, 27)
+        out = torch.empty_like(x0)
+        nat.check(nat.lib().gb_conv3d_forward_pair(
+            nat.ptr(x0), nat.ptr(x1), nat.ptr(wb), nat.ptr(out), x0.shape[0], self._n(gd),
+            (ctypes.c_int * 3)(*[int(p) for p in gd.pbc_c]), nat.stream_of(x0)),
+            'gb_conv3d_forward_pair')
+        return out
+
     def conv_bwd_w(self, x, dy, w32, gd):
         cout, cin, _ = w32.shape
         dw = torch.zeros_like(w32)
@@ -168,26 +179,33 @@ class ConvNet:
         return out.reshape(lead + tuple(out.shape[-3:]))
 
     # -------------------------------------------------------------- network
-    def forward(self, R, keep=False):
-        """R: (nb, n0, n1, n2) any float dtype -> (nb, n0, n1, n2) FP32."""
+    def forward(self, R, keep=False, scale=1.0):
+        """R: (nb, n0, n1, n2) any float dtype -> scale * net(R), (nb, n0, n1, n2)
+        FP32.  The network is linear and homogeneous, so inference runs on R
+        as it is (FP32 accumulation does not care about the overall scale);
+        training (keep=True) normalises every band to unit RMS first, which
+        keeps the per-band loss weights independent of the residual size.
+        `scale` is folded into the last convolution's weights."""
         p = self.params
         nb = R.shape[0]
         x = R.to(torch.float32)
-        s = x.reshape(nb, -1).pow(2).mean(1).sqrt().clamp_min(1e-30)
-        x = (x / s.reshape(-1, 1, 1, 1))[:, None].contiguous()        # (nb, 1, n0)
+        if keep:
+            s = x.reshape(nb, -1).pow(2).mean(1).sqrt().clamp_min(1e-30)
+            x = x / s.reshape(-1, 1, 1, 1)
+        x = x.reshape((nb, 1) + tuple(x.shape[1:])).contiguous()          # (nb, 1, n0)
         r1 = self.transfer(x, self.r01)                                  # (nb, 1, n1)
         a1 = self.conv(r1, p['wa'], self.gd1)                            # (nb, 16, n1)
         r2 = self.transfer(a1, self.r12)                                 # (nb, 16, n2)
         a2 = self.conv(r2, p['wb'], self.gd2)                            # (nb, 16, n2)
-        u1 = self.transfer(a2, self.i21) + a1                            # (nb, 16, n1)
+        u1 = torch.empty_like(a1)                                        # Interp(a2) + a1
+        self.i21.apply_axpy(self._flat(a2), self._flat(u1), 1.0, self._flat(a1), 1.0)
         b1 = self.conv(u1, p['wc'], self.gd1)                            # (nb, 1, n1)
         z = self.transfer(b1, self.i10)                                  # (nb, 1, n0)
-        y = self.conv(z, p['wp'], self.gd0)
-        self.conv(x, p['w0'], self.gd0, out=y, accumulate=True)
-        out = y[:, 0] * s.reshape(-1, 1, 1, 1)
+        y = self.conv_pair(z, x, p['wp'] * scale, p['w0'] * scale, self.gd0)
         if keep:
             self._cache = dict(x=x, s=s, r1=r1, r2=r2, u1=u1, z=z)
-        return out
+            return y[:, 0] * s.reshape(-1, 1, 1, 1)
+        return y[:, 0]
 
     def backward(self, g_out):
         """Gradients of the loss w.r.t. the four weight tensors, given
@@ -363,11 +381,11 @@ class LearnedPreconditioner:
         if R.ndim == 3:
             o = None if out is None else out[None]
             return self(R[None], kpt, out=o)[0]
-        yn = self.net.forward(R)
-        y = (yn * self.step).to(R.dtype)
+        y = self.net.forward(R, scale=self.step)
         k = min(self.nprobe, R.shape[0])
-        probe = (self.multigrid(R[:k].contiguous(), kpt) / self.step).to(torch.float32)
-        dev = self.net.relative_error_from(yn[:k], probe).max().to(torch.float64)
+        probe = self.multigrid(R[:k].contiguous(), kpt).to(torch.float32)
+        dev = self.net.relative_error_from(y[:k], probe).max().to(torch.float64)
+        y = y.to(R.dtype)
         self.deviation.copy_(torch.maximum(self.deviation, dev))
         bad = ~torch.isfinite(dev) | (dev > self.tolerance)
         self.failed.logical_or_(bad)

@@ -463,25 +463,37 @@ class _GraphedIteration:
         self.eps = torch.empty(nb, dtype=torch.float64, device=self.psit.device)
         self.V = torch.empty((nb, nb), dtype=wide, device=self.psit.device)
         self.pool = torch.cuda.graph_pool_handle()
-        torch.cuda.synchronize()
+        # capture on a side stream with capture_begin/capture_end (the
+        # torch.cuda.graph context manager would also run gc.collect() and
+        # empty the allocator's cache, whose re-filling costs far more than
+        # the capture itself)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
         self.gA = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.gA, pool=self.pool):
-            self.H, self.Htpsit = es.subspace_matrix(calc, wfs, kpt)
         self.gB = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.gB, pool=self.pool):
-            es.subspace_rotate(wfs, kpt, self.eps, self.V, self.Htpsit)
-            err = es.update_bands(calc, wfs, kpt, weights)
-            wfs.orthonormalize(kpt)
-            E = calc.total_energy(kpt) * Hartree
-            ddens = calc.update_density()
-            calc.update_hamiltonian()
-            self.psit.copy_(kpt.psit_nG)
-            if self.P is not None:
-                self.P.copy_(kpt.P_nM)
-            self.out = torch.stack([E, err, ddens, calc._judge_flag()])
+        with torch.cuda.stream(side):
+            self.gA.capture_begin(pool=self.pool)
+            self.H, self.Htpsit = es.subspace_matrix(calc, wfs, kpt)
+            self.gA.capture_end()
+            self.gB.capture_begin(pool=self.pool)
+            self._capture_b(calc, wfs, kpt, es, weights)
+            self.gB.capture_end()
+        torch.cuda.current_stream().wait_stream(side)
         kpt.psit_nG = self.psit
         kpt.P_nM = self.P
         kpt.eps_n = self.eps
+
+    def _capture_b(self, calc, wfs, kpt, es, weights):
+        es.subspace_rotate(wfs, kpt, self.eps, self.V, self.Htpsit)
+        err = es.update_bands(calc, wfs, kpt, weights)
+        wfs.orthonormalize(kpt)
+        E = calc.total_energy(kpt) * Hartree
+        ddens = calc.update_density()
+        calc.update_hamiltonian()
+        self.psit.copy_(kpt.psit_nG)
+        if self.P is not None:
+            self.P.copy_(kpt.P_nM)
+        self.out = torch.stack([E, err, ddens, calc._judge_flag()])
 
     def replay(self):
         self.gA.replay()

@@ -97,6 +97,26 @@ class _Transformer:
             nat.stream_of(input)), 'gb_transformer_apply')
         return output
 
+    def apply_axpy(self, input, output, alpha=1.0, y=None, gamma=0.0, phases=None):
+        """output = alpha * T(input) + gamma * y in one launch (y only for
+        interpolation; shaped like output)."""
+        nat.require_cuda(input, output)
+        if y is not None:
+            nat.require_cuda(y)
+            if tuple(y.shape) != tuple(output.shape) or y.dtype != output.dtype:
+                raise ValueError('y must match the output')
+        if tuple(output.shape) != tuple(input.shape[:-3]) + self.ngpout:
+            raise ValueError('output shape mismatch')
+        if input.dtype.is_complex and phases is None:
+            phases = np.ones((3, 2), complex)
+        nin = int(np.prod(input.shape[:-3], dtype=np.int64))
+        nat.check(nat.lib().gb_transformer_apply_axpy(
+            self._handle, nat.ptr(input), nat.ptr(output), nin, nat.dtype_code(input),
+            nat.phases(phases) if input.dtype.is_complex else None, float(alpha),
+            nat.ptr(y) if y is not None else None, float(gamma), nat.stream_of(input)),
+            'gb_transformer_apply_axpy')
+        return output
+
     def get_async_sizes(self):
         return (0, 1, 1)
 

@@ -113,6 +113,14 @@ int gb_transformer_new(const int64_t size_in[3], const int64_t size_out[3],
 int gb_transformer_apply(const gb_transformer* t, const void* in, void* out,
                          int64_t nin, int dtype, const double* phase_cd,
                          void* stream);
+/* out = alpha * T(in) (+ gamma * y for an interpolation, y shaped like out):
+ * the same transfer with a fused scale and addend (no reference counterpart;
+ * the V-cycle's own kernels and the learned preconditioner's skip
+ * connection use it). */
+int gb_transformer_apply_axpy(const gb_transformer* t, const void* in,
+                              void* out, int64_t nin, int dtype,
+                              const double* phase_cd, double alpha,
+                              const void* y, double gamma, void* stream);
 int gb_transformer_free(gb_transformer* t);
 
 /* ======================================================================
@@ -215,6 +223,12 @@ int gb_add_to_density(int64_t nb, const double* f_n, const void* psit_nG,
 int gb_conv3d_forward(const float* x, const void* w_bf16, float* y,
                       int64_t nb, int cin, int cout, const int64_t n_c[3],
                       const int pbc_c[3], int accumulate, void* stream);
+/* y = conv(x0, w[0][0]) + conv(x1, w[0][1]) for single-channel x0, x1, y
+ * (nb, n0, n1, n2) FP32 and BF16 w [1][2][27]: the network's two level-0
+ * convolutions in one pass. */
+int gb_conv3d_forward_pair(const float* x0, const float* x1, const void* w_bf16,
+                           float* y, int64_t nb, const int64_t n_c[3],
+                           const int pbc_c[3], void* stream);
 int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw,
                               int64_t nb, int cin, int cout,
                               const int64_t n_c[3], const int pbc_c[3],
