@@ -346,12 +346,14 @@ def network_benchmark(args):
     """The learned preconditioner's forward pass on its production shape:
     160 FP32 residuals of the 56^3 periodic Si64 grid (h = 0.194 A), the
     network initialised from the V-cycle; CUDA events around `steps` passes
-    after `warmup` untimed ones, next to the fused V-cycle on the same data."""
+    after `warmup` untimed ones: the layer-by-layer form (the one training
+    differentiates), the folded inference form (FoldedNet, what the SCF
+    runs on periodic grids) and the fused V-cycle on the same data."""
     import torch
     from gpaw_b200.grid_descriptor import GridDescriptor
     from gpaw_b200.fd_operators import Laplace
     from gpaw_b200.preconditioner import Preconditioner
-    from gpaw_b200.learned import ConvNet
+    from gpaw_b200.learned import ConvNet, FoldedNet
     cell = 10.86 / BOHR
     gd = GridDescriptor((56, 56, 56), (cell, cell, cell), True)
     mg = Preconditioner(gd, Laplace(gd, -0.5, 3), float)
@@ -371,8 +373,10 @@ def network_benchmark(args):
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / args.steps
+    folded = FoldedNet(net, scale=mg.step)
     out = {'workload': 'learned preconditioner forward, 160 x 56^3 FP32 residuals',
-           'network_ms': round(timed(lambda: net.forward(R)), 4),
+           'network_ms': round(timed(lambda: net.forward(R, scale=mg.step)), 4),
+           'network_folded_ms': round(timed(lambda: folded.forward(R)), 4),
            'vcycle_ms': round(timed(lambda: mg(R)), 4)}
     print(json.dumps(out))
 

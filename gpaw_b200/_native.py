@@ -76,6 +76,19 @@ _SIGNATURES = {
                              c_int64, c_int, c_void_p, c_void_p]),
     'gb_band_gram': (c_int, [c_int64, c_int, c_int64, c_void_p, c_int64,
                              c_int64, c_int, c_void_p, c_void_p]),
+    'gb_band_gram_tc_workspace': (c_int, [c_int64, c_int64, c_int64, POINTER(c_int64)]),
+    'gb_band_gram_tc': (c_int, [c_int64, c_int64, c_int64, c_void_p, c_int64, c_void_p,
+                                c_int64, c_double, c_void_p, c_int64, c_void_p, c_int64,
+                                c_void_p]),
+    'gb_tf32_split': (c_int, [c_int64, c_int64, c_void_p, c_int64, c_void_p, c_void_p,
+                              c_int64, c_void_p]),
+    'gb_band_rotate_tc': (c_int, [c_int64, c_int64, c_int64, c_void_p, c_void_p, c_int64,
+                                  c_void_p, c_int64, ctypes.c_float, c_void_p, c_int64,
+                                  c_void_p, c_int64, c_void_p]),
+    'gb_learned_fold_fine': (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                                     c_void_p, c_int64, c_void_p, c_void_p]),
+    'gb_learned_fold_stride': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p,
+                                       c_void_p]),
     'gb_small_solve': (c_int, [c_int64, c_int, c_void_p, c_void_p, c_void_p,
                                c_void_p, c_void_p]),
     'gb_band_combine': (c_int, [c_int64, c_int64, c_int, c_void_p, c_void_p,

@@ -658,6 +658,8 @@ int gb_set_stencil_path(int mode) {
 int gb_device_errors(int clear, int* code) {
   if (!code) return gb::fail(GB_E_INVALID, "gb_device_errors: null pointer");
   *code = gb::device_error_flag(clear);
+  const int tc = gb::band_tc_error_flag(clear);
+  if (!*code) *code = tc;
   return GB_OK;
 }
 

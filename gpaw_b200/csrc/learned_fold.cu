@@ -1,0 +1,287 @@
+// Folded inference of the learned preconditioner on periodic grids (no
+// reference counterpart: the network stands in for the V-cycle of
+// c/fd_preconditioner.c).
+//
+// The network is linear, so on a periodic grid its layers compose exactly
+// into three stencils over single-channel inputs plus the 16-channel
+// level-2 convolution (which stays as it is):
+//
+//   r2[c][I] = sum_{d in [-2,2]^3} Q[c][d] r1[2I + d]           fold_stride
+//              (Q = restriction o conv_a: 1 -> 16 channels, stride 2)
+//   b1[p]    = sum_{d in [-2,2]^3} C1[d] r1[p + d]               fold_fine<2, 16>
+//            + sum_c sum_{e in {-1,0,1}^3} G[c][(p mod 2) - 2e] a2[c][p/2 + e]
+//              (C1 = conv_c o conv_a; G = conv_c o interpolation)
+//   y[p]     = sum_{d in [-1,1]^3} W0[d] x[p + d]                fold_fine<1, 1>
+//            + sum_{e} H[(p mod 2) - 2e] b1[p/2 + e]
+//              (H = conv_p o interpolation, the step folded in)
+//
+// so the 16-channel level-1 tensors (and the interpolated level-0 grid) are
+// never written.  Index conventions: fine point p sits on coarse point p/2
+// (periodic grids of even size); G and H are stored [c][tx][ty][tz] with
+// t = d + 2 in 0..5 (d = (p mod 2) - 2e in -2..3; t = 5 is zero).  The
+// composite weights are extracted on the host side by applying the unfolded
+// network to delta inputs, so they inherit its BF16 weights and transfer
+// coefficients exactly.
+//
+// Both kernels read their neighbourhoods through L1 (__ldg) with the lanes
+// of a warp along a grid row (coalesced), keep the weights in shared memory
+// and give every thread a column of 4 output rows (fold_fine: each loaded
+// input row serves all of them) or two neighbouring coarse points with all
+// 16 channels (fold_stride).  FP32 throughout.
+#include <algorithm>
+#include "internal.cuh"
+
+namespace gb {
+namespace {
+
+// periodic index for -n <= x < 2n (every offset these kernels form stays in
+// that range: rows of at least PXF + 2 points are required)
+__device__ __forceinline__ int pw(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
+
+struct FoldArgs {
+  const float* xf;   // (nb, n0, n1, n2)
+  const float* xc;   // (nb, CC, n0/2, n1/2, n2/2)
+  float* y;          // (nb, n0, n1, n2)
+  const float* F;    // (2 RH + 1)^3
+  const float* G;    // CC x 216
+  int64_t nb;
+  int n0, n1, n2;
+};
+
+constexpr int PXF = 8;   // minimum row length beyond the 2-point halo
+constexpr int JB = 4;    // output rows per thread (axis 1)
+
+// launch: block (32, 8) = 32 points of a row x 8 row blocks, grid
+// (row chunks x row-block groups, planes, bands): no index divisions beyond
+// one small one per thread; offsets inside a band are 32-bit
+// thread = one point k of a row (lanes run along the row: coalesced loads)
+// and JB consecutive rows j0 .. j0 + JB - 1 of one plane i; every input row
+// it loads serves all the outputs it touches
+template <int RH, int CC>
+__global__ void __launch_bounds__(256, CC > 1 ? 2 : 3) fold_fine_kernel(const FoldArgs a) {
+  constexpr int FW = 2 * RH + 1;
+  constexpr int NR = JB + 2 * RH;          // input rows per plane
+  __shared__ float sF[FW * FW * FW];
+  __shared__ float sG[CC * 216];
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  for (int e = tid; e < FW * FW * FW; e += 256) sF[e] = a.F[e];
+  for (int e = tid; e < CC * 216; e += 256) sG[e] = a.G[e];
+  __syncthreads();
+  const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
+  const int m0 = n0 >> 1, m1 = n1 >> 1, m2 = n2 >> 1;
+  const int nkx = (n2 + 31) >> 5;
+  const int k = (blockIdx.x % nkx) * 32 + threadIdx.x;
+  const int j0 = ((blockIdx.x / nkx) * 8 + threadIdx.y) * JB;
+  const int i = blockIdx.y;
+  const int64_t b = blockIdx.z;
+  if (k >= n2 || j0 >= n1) return;
+  const int plane = n1 * n2, cplane = m1 * m2;
+  float acc[JB];
+#pragma unroll
+  for (int q = 0; q < JB; ++q) acc[q] = 0.f;
+  int kk[FW];
+#pragma unroll
+  for (int m = 0; m < FW; ++m) kk[m] = pw(k - RH + m, n2);
+  const float* xb = a.xf + b * n0 * (int64_t)plane;
+#pragma unroll 1
+  for (int dx = -RH; dx <= RH; ++dx) {
+    const float* pl = xb + pw(i + dx, n0) * plane;
+    const float* f = sF + (dx + RH) * FW * FW;
+    float fr[FW * FW];
+#pragma unroll
+    for (int t = 0; t < FW * FW; ++t) fr[t] = f[t];
+#pragma unroll
+    for (int rr = 0; rr < NR; ++rr) {
+      const float* rp = pl + pw(j0 - RH + rr, n1) * n2;
+      float v[FW];
+#pragma unroll
+      for (int m = 0; m < FW; ++m) v[m] = __ldg(rp + kk[m]);
+#pragma unroll
+      for (int q = 0; q < JB; ++q) {
+        const int dy = rr - RH - q;          // compile-time after unrolling
+        if (dy < -RH || dy > RH) continue;
+#pragma unroll
+        for (int m = 0; m < FW; ++m) acc[q] = fmaf(fr[(dy + RH) * FW + m], v[m], acc[q]);
+      }
+    }
+  }
+  // coarse part: coarse rows j0/2 - 1 .. j0/2 + JB/2, columns k/2 - 1 .. k/2 + 1;
+  // the weights one (channel, plane offset) needs -- 5 row parities x 3
+  // column offsets for this thread's column parity -- go to registers once
+  const int I0 = i >> 1, J0 = j0 >> 1, K0 = k >> 1;
+  const int px = i & 1, pz = k & 1;
+  int kc[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) kc[m] = pw(K0 - 1 + m, m2);
+  int crow[JB / 2 + 2];
+#pragma unroll
+  for (int rr = 0; rr < JB / 2 + 2; ++rr) crow[rr] = pw(J0 - 1 + rr, m1) * m2;
+  const float* cb = a.xc + b * CC * (int64_t)m0 * cplane;
+#pragma unroll 1
+  for (int c = 0; c < CC; ++c) {
+    const float* cc = cb + c * m0 * cplane;
+    const float* gc = sG + c * 216;
+#pragma unroll
+    for (int ex = -1; ex <= 1; ++ex) {
+      const int tx = px - 2 * ex + 2;
+      if (tx > 4) continue;
+      float wz[5][3];                        // [ty][ez + 1]; tz = pz - 2 ez + 2
+#pragma unroll
+      for (int ty = 0; ty < 5; ++ty)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          const int tz = pz - 2 * (m - 1) + 2;
+          wz[ty][m] = tz <= 4 ? gc[(tx * 6 + ty) * 6 + tz] : 0.f;
+        }
+      const float* cpl = cc + pw(I0 + ex, m0) * cplane;
+#pragma unroll
+      for (int rr = 0; rr < JB / 2 + 2; ++rr) {
+        float v[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) v[m] = __ldg(cpl + crow[rr] + kc[m]);
+#pragma unroll
+        for (int q = 0; q < JB; ++q) {
+          // output row j0 + q sits on coarse row J0 + q/2 with parity q & 1
+          const int ey = rr - 1 - q / 2;
+          if (ey < -1 || ey > 1) continue;
+          const int ty = (q & 1) - 2 * ey + 2;   // compile-time
+          if (ty > 4) continue;
+#pragma unroll
+          for (int m = 0; m < 3; ++m) acc[q] = fmaf(wz[ty][m], v[m], acc[q]);
+        }
+      }
+    }
+  }
+  float* yp = a.y + b * n0 * (int64_t)plane + i * plane + k;
+#pragma unroll
+  for (int q = 0; q < JB; ++q)
+    if (j0 + q < n1) yp[(j0 + q) * n2] = acc[q];
+}
+
+// r2[b][c][I] = sum_d Q[d][c] r1[b][2I + d], d in [-2, 2]^3, 16 channels
+struct StrideArgs {
+  const float* x;    // (nb, n0, n1, n2) fine (level-1) grid
+  float* y;          // (nb, 16, n0/2, n1/2, n2/2)
+  const float* Q;    // [125][16]
+  int64_t nb;
+  int n0, n1, n2;
+};
+
+// thread = two neighbouring coarse points (K, K + 1) of a row, all 16
+// channels: the 7 fine columns they read and every weight load are shared
+__global__ void __launch_bounds__(256) fold_stride_kernel(const StrideArgs a) {
+  __shared__ __align__(16) float sQ[125 * 16];
+  for (int e = threadIdx.x; e < 125 * 16; e += blockDim.x) sQ[e] = a.Q[e];
+  __syncthreads();
+  const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
+  const int m0 = n0 >> 1, m1 = n1 >> 1, m2 = n2 >> 1;
+  const int mh = (m2 + 1) / 2;                      // point pairs per coarse row
+  const int64_t mpts = (int64_t)m0 * m1 * m2;
+  const int64_t plane = (int64_t)n1 * n2;
+  const int64_t total = a.nb * m0 * (int64_t)m1 * mh;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int K = (int)(e % mh) * 2;
+    int64_t r = e / mh;
+    const int J = (int)(r % m1);
+    r /= m1;
+    const int I = (int)(r % m0);
+    const int64_t b = r / m0;
+    const bool two = K + 1 < m2;
+    float acc0[16], acc1[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) { acc0[c] = 0.f; acc1[c] = 0.f; }
+    int kk[7];
+#pragma unroll
+    for (int m = 0; m < 7; ++m) kk[m] = pw(2 * K - 2 + m, n2);
+    const float* xb = a.x + b * n0 * plane;
+#pragma unroll 1
+    for (int dx = 0; dx < 5; ++dx) {
+      const float* pl = xb + pw(2 * I + dx - 2, n0) * plane;
+#pragma unroll 1
+      for (int dy = 0; dy < 5; ++dy) {
+        const float* rp = pl + (int64_t)pw(2 * J + dy - 2, n1) * n2;
+        float w[7];
+#pragma unroll
+        for (int m = 0; m < 7; ++m) w[m] = __ldg(rp + kk[m]);
+        const float4* q4 = reinterpret_cast<const float4*>(sQ + ((dx * 5 + dy) * 5) * 16);
+#pragma unroll
+        for (int dz = 0; dz < 5; ++dz) {
+#pragma unroll
+          for (int c4 = 0; c4 < 4; ++c4) {
+            const float4 q = q4[dz * 4 + c4];
+            acc0[4 * c4] = fmaf(q.x, w[dz], acc0[4 * c4]);
+            acc0[4 * c4 + 1] = fmaf(q.y, w[dz], acc0[4 * c4 + 1]);
+            acc0[4 * c4 + 2] = fmaf(q.z, w[dz], acc0[4 * c4 + 2]);
+            acc0[4 * c4 + 3] = fmaf(q.w, w[dz], acc0[4 * c4 + 3]);
+            acc1[4 * c4] = fmaf(q.x, w[dz + 2], acc1[4 * c4]);
+            acc1[4 * c4 + 1] = fmaf(q.y, w[dz + 2], acc1[4 * c4 + 1]);
+            acc1[4 * c4 + 2] = fmaf(q.z, w[dz + 2], acc1[4 * c4 + 2]);
+            acc1[4 * c4 + 3] = fmaf(q.w, w[dz + 2], acc1[4 * c4 + 3]);
+          }
+        }
+      }
+    }
+    float* yb = a.y + b * 16 * mpts + ((int64_t)I * m1 + J) * m2 + K;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      yb[c * mpts] = acc0[c];
+      if (two) yb[c * mpts + 1] = acc1[c];
+    }
+  }
+}
+
+template <typename KernelT>
+int launch_fine(KernelT k, const FoldArgs& a, const char* what, cudaStream_t st) {
+  const int nkx = (a.n2 + 31) / 32;
+  const int njb = (a.n1 + JB - 1) / JB;
+  const dim3 grid((unsigned)(nkx * ((njb + 7) / 8)), (unsigned)a.n0, (unsigned)a.nb);
+  k<<<grid, dim3(32, 8), 0, st>>>(a);
+  return check_launch(what);
+}
+
+template <typename KernelT, typename ArgsT>
+int launch_grid(KernelT k, const ArgsT& a, int64_t work, const char* what, cudaStream_t st) {
+  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)sm_count() * 16));
+  k<<<(unsigned)blocks, 256, 0, st>>>(a);
+  return check_launch(what);
+}
+
+}  // namespace
+}  // namespace gb
+
+using namespace gb;
+
+extern "C" {
+
+int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* xc, const float* G, int cc,
+                         float* y, int64_t nb, const int64_t n_c[3], void* stream) {
+  GB_REQUIRE(xf && F && y && n_c && nb >= 0, "gb_learned_fold_fine: bad arguments");
+  if (nb == 0) return GB_OK;
+  GB_REQUIRE(n_c[2] >= PXF + 2, "gb_learned_fold_fine: rows shorter than 10 points");
+  GB_REQUIRE(n_c[0] >= 2 && n_c[1] >= 2 && n_c[2] >= 2 && n_c[0] % 2 == 0 && n_c[1] % 2 == 0 &&
+                 n_c[2] % 2 == 0 && n_c[0] < (1 << 20) && n_c[1] < (1 << 20) && n_c[2] < (1 << 20),
+             "gb_learned_fold_fine: needs even grid sizes (periodic coarsening)");
+  GB_REQUIRE(xc && G, "gb_learned_fold_fine: missing coarse input or weights");
+  GB_REQUIRE(nb < 65536 && n_c[0] * n_c[1] * n_c[2] * (cc > 1 ? cc : 1) < ((int64_t)1 << 31),
+             "gb_learned_fold_fine: too many grids or points per grid");
+  FoldArgs a{xf, xc, y, F, G, nb, (int)n_c[0], (int)n_c[1], (int)n_c[2]};
+  cudaStream_t st = (cudaStream_t)stream;
+  if (rh == 1 && cc == 1) return launch_fine(fold_fine_kernel<1, 1>, a, "fold_fine_kernel<1,1>", st);
+  if (rh == 2 && cc == 16) return launch_fine(fold_fine_kernel<2, 16>, a, "fold_fine_kernel<2,16>", st);
+  return fail(GB_E_UNSUPPORTED, "gb_learned_fold_fine: (rh, cc) not in {(1, 1), (2, 16)}");
+}
+
+int gb_learned_fold_stride(const float* x, const float* Q, float* y, int64_t nb, const int64_t n_c[3],
+                           void* stream) {
+  GB_REQUIRE(x && Q && y && n_c && nb >= 0, "gb_learned_fold_stride: bad arguments");
+  if (nb == 0) return GB_OK;
+  GB_REQUIRE(n_c[0] >= 2 && n_c[1] >= 2 && n_c[2] >= 2 && n_c[0] % 2 == 0 && n_c[1] % 2 == 0 &&
+                 n_c[2] % 2 == 0 && n_c[0] < (1 << 20) && n_c[1] < (1 << 20) && n_c[2] < (1 << 20),
+             "gb_learned_fold_stride: needs even grid sizes (periodic coarsening)");
+  StrideArgs a{x, y, Q, nb, (int)n_c[0], (int)n_c[1], (int)n_c[2]};
+  const int64_t work = nb * (n_c[0] / 2) * (n_c[1] / 2) * ((n_c[2] / 2 + 1) / 2);
+  return launch_grid(fold_stride_kernel, a, work, "fold_stride_kernel", (cudaStream_t)stream);
+}
+
+}  // extern "C"

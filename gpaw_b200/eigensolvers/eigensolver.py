@@ -8,14 +8,15 @@ atoms.  H_nn = dv psi^H (T + v) psi + P^* dH P^T is accumulated in FP64 and
 diagonalised in FP64 (torch.linalg.eigh on the device); psi, (T + v) psi and
 P are rotated with GEMMs in the working precision.  Eigenvalues stay on the
 device (kpt.eps_n, FP64), so an iteration needs no host round trip except
-the eigensolver of the subspace matrix itself.
+the eigensolver of the subspace matrix itself.  FP32 real wave functions take
+the tensor-core band GEMMs (gpaw_b200.bandops.gram_tc / rotate_tc).
 """
 from __future__ import annotations
 
 import numpy as np
 import torch
 
-from gpaw_b200.bandops import band_combine
+from gpaw_b200.bandops import band_combine, rotate_tc, tf32_split
 
 
 class Eigensolver:
@@ -86,6 +87,21 @@ class Eigensolver:
         psit = kpt.psit_nG
         nb = psit.shape[0]
         # phi_k = sum_m V[m, k] psi_m
+        if psit.dtype == torch.float32:
+            # FP32 real: tensor-core rotations sharing one TF32 split of
+            # V^T - I (psi + (V^T - I) psi: near convergence V is close to
+            # the identity, so the FP32 truncation of the tensor core stays
+            # in the small correction)
+            eye = torch.eye(nb, dtype=V.dtype, device=V.device)
+            hi, lo = tf32_split(V.T - eye)
+            new = rotate_tc((hi, lo, nb), psit, identity_split=True)
+            if new is not None:
+                kpt.psit_nG = new
+                self.Htpsit_nG = rotate_tc((hi, lo, nb), Htpsit, identity_split=True)
+                if kpt.P_nM is not None:
+                    kpt.P_nM = V.T.to(kpt.P_nM.dtype) @ kpt.P_nM
+                kpt.eps_n = eps
+                return
         U = V.T.to(wfs.dtype)
         kpt.psit_nG = (U @ psit.reshape(nb, -1)).reshape(psit.shape)
         self.Htpsit_nG = (U @ Htpsit.reshape(nb, -1)).reshape(psit.shape)

@@ -355,6 +355,139 @@ class PairRecorder:
         return torch.cat(self.R), torch.cat(self.T)
 
 
+class FoldedNet:
+    """Inference form of a ConvNet on a periodic grid of even sizes (all
+    three levels): the linear layers folded into composite stencils
+    (gb_learned_fold_stride / gb_learned_fold_fine), with the 16-channel
+    level-2 convolution kept as it is.  Per forward:
+
+        r1 = Restrict(x)                      (transformer kernel)
+        r2 = Q *2 r1                          (stride-2 5^3 stencil, 1 -> 16)
+        a2 = conv_b(r2)                       (16 -> 16, unchanged)
+        b1 = C1 * r1 + G (x) a2               (5^3 stencil + parity stencil)
+        y  = W0 * x  + H (x) b1               (3^3 stencil + parity stencil)
+
+    instead of four transfers and five convolutions over 16-channel level-1
+    tensors.  The composite weights come from applying the unfolded network
+    (its own kernels and BF16 weights) to delta inputs on a small periodic
+    grid, so both forms compute the same linear map up to FP32 rounding;
+    every probe also checks that no weight falls outside the windows the
+    kernels read."""
+
+    PROBE_N = 32
+
+    @staticmethod
+    def applies(gd):
+        """Periodic, every size divisible by 4 and the level-1 rows at least
+        10 points long (the stencils' wrap-around arithmetic)."""
+        n = np.asarray(gd.n_c)
+        return bool(np.all(gd.pbc_c) and np.all(n % 4 == 0) and n[2] >= 20)
+
+    def __init__(self, net: ConvNet, scale=1.0):
+        gd = net.gd0
+        if not self.applies(gd):
+            raise ValueError('FoldedNet: needs a periodic grid, sizes divisible by 4, >= 20')
+        self.net = net
+        self.scale = float(scale)
+        from gpaw_b200.grid_descriptor import GridDescriptor
+        N = self.PROBE_N
+        gdp = GridDescriptor((N, N, N), np.eye(3) * N * 0.4, True, device=net.device)
+        pn = ConvNet(gdp, device=net.device, params=net.params)
+        self._extract(pn)
+
+    @staticmethod
+    def _window(t, centre, lo, hi, what):
+        """t (..., M, M, M) response around `centre` (3 ints): returns the
+        block of offsets lo..hi per axis and checks that the rest is zero."""
+        c0, c1, c2 = centre
+        blk = t[..., c0 + lo:c0 + hi + 1, c1 + lo:c1 + hi + 1, c2 + lo:c2 + hi + 1].clone()
+        rest = t.clone()
+        rest[..., c0 + lo:c0 + hi + 1, c1 + lo:c1 + hi + 1, c2 + lo:c2 + hi + 1] = 0
+        scale = blk.abs().max().clamp_min(1e-30)
+        if rest.abs().max() > 1e-6 * scale:
+            raise RuntimeError(f'FoldedNet: {what} reaches beyond its stencil window')
+        return blk
+
+    def _extract(self, pn):
+        p = pn.params
+        dev = pn.device
+        N1 = pn.gd1.n_c[0]          # level-1 probe size
+        c1 = N1 // 2
+        # C1 = conv_c o conv_a on level 1: b1[p] = sum_d C1[d] r1[p + d]
+        r1 = torch.zeros((1, 1, N1, N1, N1), dtype=torch.float32, device=dev)
+        r1[0, 0, c1, c1, c1] = 1.0
+        a1 = pn.conv(r1, p['wa'], pn.gd1)
+        b1 = pn.conv(a1, p['wc'], pn.gd1)[0, 0]
+        blk = self._window(b1, (c1, c1, c1), -2, 2, 'conv_c o conv_a')
+        self.C1 = blk.flip(0, 1, 2).contiguous().reshape(-1)           # C1[d] = b1[c - d]
+        # Q = Restrict o conv_a: r2[c][I] = sum_d Q[c][d] r1[2I + d]; one probe
+        # per parity class of the delta position
+        N2 = pn.gd2.n_c[0]
+        Q = torch.zeros((16, 5, 5, 5), dtype=torch.float64, device=dev)
+        seen = torch.zeros((5, 5, 5), dtype=torch.bool, device=dev)
+        par = [(a, b, c) for a in (0, 1) for b in (0, 1) for c in (0, 1)]
+        r1 = torch.zeros((8, 1, N1, N1, N1), dtype=torch.float32, device=dev)
+        for k, (a, b, c) in enumerate(par):
+            r1[k, 0, c1 + a, c1 + b, c1 + c] = 1.0
+        r2 = pn.transfer(pn.conv(r1, p['wa'], pn.gd1), pn.r12)          # (8, 16, N2^3)
+        I = torch.arange(N2, device=dev)
+        for k, (a, b, c) in enumerate(par):
+            q = torch.tensor([c1 + a, c1 + b, c1 + c], device=dev)
+            d = [((q[ax] - 2 * I + N1 // 2) % N1) - N1 // 2 for ax in range(3)]   # wrapped offsets
+            inside = [(dd.abs() <= 2) for dd in d]
+            resp = r2[k].double()
+            mask = inside[0][:, None, None] & inside[1][None, :, None] & inside[2][None, None, :]
+            if resp[:, ~mask].abs().max() > 1e-6 * resp.abs().max().clamp_min(1e-30):
+                raise RuntimeError('FoldedNet: restrict o conv_a reaches beyond its stencil window')
+            ix = [torch.nonzero(m).flatten() for m in inside]
+            sub = resp[:, ix[0]][:, :, ix[1]][:, :, :, ix[2]]
+            dx, dy, dz = [(d[ax][ix[ax]] + 2) for ax in range(3)]
+            Q[:, dx[:, None, None], dy[None, :, None], dz[None, None, :]] = sub
+            seen[dx[:, None, None], dy[None, :, None], dz[None, None, :]] = True
+        if not bool(seen.all()):
+            raise RuntimeError('FoldedNet: the restriction probes did not cover every offset')
+        self.Q = Q.reshape(16, 125).T.contiguous().to(torch.float32)   # [125][16]
+        # G = conv_c o Interp(2 -> 1): b1[p] = sum_c G[c][p - 2J] a2[c][J]
+        J0 = N2 // 2
+        a2 = torch.zeros((16, 16, N2, N2, N2), dtype=torch.float32, device=dev)
+        for c in range(16):
+            a2[c, c, J0, J0, J0] = 1.0
+        b1 = pn.conv(pn.transfer(a2, pn.i21), p['wc'], pn.gd1)[:, 0]     # (16, N1^3)
+        blk = self._window(b1, (2 * J0,) * 3, -2, 3, 'conv_c o interpolation')
+        self.G = blk.contiguous().reshape(16, 216)
+        # H = conv_p o Interp(1 -> 0), the step folded in; W0 = step * w0
+        # (BF16-rounded like the unfolded level-0 convolution)
+        N0 = pn.gd0.n_c[0]
+        b1 = torch.zeros((1, 1, N1, N1, N1), dtype=torch.float32, device=dev)
+        b1[0, 0, c1, c1, c1] = 1.0
+        y = pn.conv(pn.transfer(b1, pn.i10), p['wp'] * self.scale, pn.gd0)[0, 0]
+        blk = self._window(y, (2 * c1,) * 3, -2, 3, 'conv_p o interpolation')
+        self.H = blk.contiguous().reshape(216)
+        self.W0 = (p['w0'] * self.scale).to(torch.bfloat16).to(torch.float32).reshape(27).contiguous()
+
+    def forward(self, R):
+        """scale * net(R) for R (nb, n0, n1, n2): FP32 out."""
+        net = self.net
+        x = R.to(torch.float32).contiguous()
+        nb = x.shape[0]
+        st = nat.stream_of(x)
+        r1 = net.r01.apply(x)
+        n1 = nat.i64(net.gd1.n_c)
+        r2 = torch.empty((nb, 16) + tuple(net.gd2.n_c), dtype=torch.float32, device=x.device)
+        nat.check(nat.lib().gb_learned_fold_stride(nat.ptr(r1), nat.ptr(self.Q), nat.ptr(r2), nb,
+                                                   n1, st), 'gb_learned_fold_stride')
+        a2 = net.conv(r2, net.params['wb'], net.gd2)
+        b1 = torch.empty_like(r1)
+        nat.check(nat.lib().gb_learned_fold_fine(nat.ptr(r1), nat.ptr(self.C1), 2, nat.ptr(a2),
+                                                 nat.ptr(self.G), 16, nat.ptr(b1), nb, n1, st),
+                  'gb_learned_fold_fine')
+        y = torch.empty_like(x)
+        nat.check(nat.lib().gb_learned_fold_fine(nat.ptr(x), nat.ptr(self.W0), 1, nat.ptr(b1),
+                                                 nat.ptr(self.H), 1, nat.ptr(y), nb,
+                                                 nat.i64(net.gd0.n_c), st), 'gb_learned_fold_fine')
+        return y
+
+
 class LearnedPreconditioner:
     """Drop-in for Preconditioner.__call__(R, kpt): the network's correction
     (scaled by the multigrid step of this grid), with the multigrid as judge
@@ -376,12 +509,17 @@ class LearnedPreconditioner:
         self.nprobe = nprobe
         self.failed = torch.zeros((), dtype=torch.bool, device=net.device)
         self.deviation = torch.zeros((), dtype=torch.float64, device=net.device)
+        # periodic grids (sizes divisible by 4): the folded inference form
+        self.folded = None
+        if FoldedNet.applies(net.gd0):
+            self.folded = FoldedNet(net, scale=self.step)
 
     def __call__(self, R, kpt=None, ekin=None, out=None):
         if R.ndim == 3:
             o = None if out is None else out[None]
             return self(R[None], kpt, out=o)[0]
-        y = self.net.forward(R, scale=self.step)
+        y = (self.folded.forward(R) if self.folded is not None
+             else self.net.forward(R, scale=self.step))
         k = min(self.nprobe, R.shape[0])
         probe = self.multigrid(R[:k].contiguous(), kpt).to(torch.float32)
         dev = self.net.relative_error_from(y[:k], probe).max().to(torch.float64)

@@ -16,7 +16,7 @@ import torch
 
 from gpaw_b200.fd_operators import Laplace
 from gpaw_b200.lfc import LFC
-from gpaw_b200.bandops import band_dots, band_gram
+from gpaw_b200.bandops import band_dots, band_gram, gram_tc, rotate_tc
 
 REAL_OF = {torch.float64: torch.float64, torch.float32: torch.float32,
            torch.complex128: torch.float64, torch.complex64: torch.float32}
@@ -79,6 +79,13 @@ class FDWaveFunctions:
         subspace-Hamiltonian matrices feed Cholesky and eigh, which stay FP64,
         so their sums over grid points are accumulated in FP64 even when
         the wave functions are FP32 (the operands are widened on the fly)."""
+        if a_nG.dtype == torch.float32 and b_nG.dtype == torch.float32:
+            # FP32 real: tensor-core Gram (three-product TF32 split), the
+            # diagonal from FP64-accumulated dots
+            C = gram_tc(a_nG, b_nG, self.gd.dv,
+                        exact_diagonal=a_nG.shape[0] == b_nG.shape[0])
+            if C is not None:
+                return C
         wide = torch.complex128 if self.dtype.is_complex else torch.float64
         A = a_nG.reshape(a_nG.shape[0], -1).to(wide)
         B = b_nG.reshape(b_nG.shape[0], -1).to(wide)
@@ -93,9 +100,13 @@ class FDWaveFunctions:
         Linv = torch.linalg.solve_triangular(
             L, torch.eye(L.shape[0], dtype=L.dtype, device=L.device), upper=False)
         # psi_n <- sum_m Linv[n, m]^* psi_m  (S = L L^H, <phi|phi> = 1)
-        C = Linv.conj().to(self.dtype)
         nb = psit.shape[0]
-        kpt.psit_nG = (C @ psit.reshape(nb, -1)).reshape(psit.shape)
+        y = (rotate_tc(Linv, psit, identity_split=True)
+             if psit.dtype == torch.float32 else None)
+        if y is None:
+            C = Linv.conj().to(self.dtype)
+            y = (C @ psit.reshape(nb, -1)).reshape(psit.shape)
+        kpt.psit_nG = y
         kpt.P_nM = self.projections(kpt.psit_nG, kpt)
 
     @staticmethod

@@ -233,6 +233,19 @@ int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw,
                               int64_t nb, int cin, int cout,
                               const int64_t n_c[3], const int pbc_c[3],
                               void* stream);
+/* Folded inference of the (linear) network on periodic grids of even size,
+ * FP32, composite weights from the caller:
+ *   fine:   y[p] = sum_{|d|<=rh} F[d] xf[p + d]
+ *                + sum_{c<cc} sum_{e in {-1,0,1}^3} G[c][(p%2) - 2e + 2] xc[c][p/2 + e]
+ *           F: (2rh+1)^3, G: cc x 6^3 ([c][tx][ty][tz]); (rh, cc) in
+ *           {(1, 1), (2, 16)}; xc (nb, cc, n/2) per axis; n2 >= 10
+ *   stride: y[c][I] = sum_{|d|<=2} Q[d][c] x[2I + d], 16 channels out,
+ *           Q [125][16], y (nb, 16, n/2) per axis */
+int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* xc,
+                         const float* G, int cc, float* y, int64_t nb,
+                         const int64_t n_c[3], void* stream);
+int gb_learned_fold_stride(const float* x, const float* Q, float* y, int64_t nb,
+                           const int64_t n_c[3], void* stream);
 
 /* ======================================================================
  * Per-band inner products of RMM-DIIS -- the gd.integrate(a_nG, b_nG) /
@@ -248,6 +261,37 @@ int gb_band_dots(int64_t nb, int64_t N, const void* a, int64_t lda,
                  void* stream);
 int gb_band_gram(int64_t nb, int k, int64_t N, const void* X, int64_t ldn,
                  int64_t ldi, int dtype, double* out, void* stream);
+/* ====================================================================
+ * Band-space GEMMs of the eigensolver on the tcgen05 tensor cores, FP32
+ * wave functions, FP32 accuracy by the three-product TF32 split
+ * (x = hi + lo, a b ~ hi hi + hi lo + lo hi).  Replace the GEMMs of
+ * gpaw/wavefunctions/fdpw.py:394-424 (overlap + inverse-Cholesky
+ * rotation), gpaw/eigensolvers/eigensolver.py:174-236 (H_nn and the
+ * subspace rotation) and gpaw/matrix.py:229-260 (the BLAS calls behind
+ * them).  Rows are 16-byte aligned (ld % 4 == 0, 16-byte aligned bases);
+ * other layouts return GB_E_UNSUPPORTED.
+ *   gram:   C[i*ldc + j] = alpha sum_{G<K} A[i*lda + G] B[j*ldb + G]
+ *           (FP64 out; `work` of gb_band_gram_tc_workspace bytes holds the
+ *           per-CTA FP64 partial sums, combined in a fixed order)
+ *   split:  hi/lo TF32 parts (FP32 containers) of an FP64 matrix,
+ *           rows x cols, zero-padded to ldd columns
+ *   rotate: Y[n*ldy + G] = sum_{k<nk} U[n][k] X[k*ldx + G]
+ *                          + beta Z[n*ldz + G]   (Z optional, may be X),
+ *           U given as its split parts Uhi/Ulo (nn x nk, leading dim ldu);
+ *           Y must not alias X or Z.  FP32 additions in the tensor core
+ *           truncate (~1e-6 relative shrink of a 160-term sum): rotating by
+ *           U - I with Z = X keeps that bias in the correction only
+ * ==================================================================== */
+int gb_band_gram_tc_workspace(int64_t na, int64_t nb, int64_t K, int64_t* bytes);
+int gb_band_gram_tc(int64_t na, int64_t nb, int64_t K, const float* A, int64_t lda,
+                    const float* B, int64_t ldb, double alpha, double* C, int64_t ldc,
+                    void* work, int64_t work_bytes, void* stream);
+int gb_tf32_split(int64_t rows, int64_t cols, const double* x, int64_t lds,
+                  float* hi, float* lo, int64_t ldd, void* stream);
+int gb_band_rotate_tc(int64_t nn, int64_t nk, int64_t K, const float* Uhi,
+                      const float* Ulo, int64_t ldu, const float* X, int64_t ldx,
+                      float beta, const float* Z, int64_t ldz, float* Y, int64_t ldy,
+                      void* stream);
 /* nb independent n x n FP64 systems A[s] x[s] = b[s] (n <= 8), the DIIS
  * solves of gpaw/eigensolvers/rmmdiis.py:175-190 and of the density mixer
  * (gpaw/mixer.py); partial pivoting; a singular system gives info[s] = 1 and
