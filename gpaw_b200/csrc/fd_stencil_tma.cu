@@ -559,22 +559,35 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st, &cs);
     if (cs == cudaStreamCaptureStatusNone) {
+      // one warm-up round, then three rounds that time every candidate once
+      // each, interleaved, keeping each candidate's fastest launch: clock
+      // ramps and the cache state left by the previous launch affect every
+      // candidate alike
       cudaEvent_t e0, e1;
       if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
-        float best_ms = 1e30f;
+        float t_c[16];
+        bool bad_c[16];
         for (int c = 0; c < nok; ++c) {
-          if (launch(c)) continue;   // warm-up run of this shape
-          cudaEventRecord(e0, st);
-          int bad = 0;
-          for (int r = 0; r < 2; ++r) bad |= launch(c);
-          cudaEventRecord(e1, st);
-          float ms = 0.f;
-          if (!bad && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
-              ms < best_ms) {
-            best_ms = ms;
+          t_c[c] = 1e30f;
+          bad_c[c] = launch(c) != 0;
+        }
+        for (int round = 0; round < 3; ++round)
+          for (int c = 0; c < nok; ++c) {
+            if (bad_c[c]) continue;
+            cudaEventRecord(e0, st);
+            bad_c[c] = launch(c) != 0;
+            cudaEventRecord(e1, st);
+            float ms = 0.f;
+            if (!bad_c[c] && cudaEventSynchronize(e1) == cudaSuccess &&
+                cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+              t_c[c] = std::min(t_c[c], ms);
+          }
+        float best_ms = 1e30f;
+        for (int c = 0; c < nok; ++c)
+          if (!bad_c[c] && t_c[c] < best_ms) {
+            best_ms = t_c[c];
             choice = c;
           }
-        }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
       }

@@ -115,6 +115,34 @@ template <typename T> struct AType { using A = double; };
 template <> struct AType<float> { using A = float; };
 template <> struct AType<float2> { using A = float; };
 
+// a row of NMAX values of A (or of the coefficients): 16-byte loads when the
+// row is full (nm == NMAX == 8) and 16-byte aligned -- a warp then reads its
+// 32 rows in two (FP32) or four (FP64) wide requests instead of 8 strided
+// ones -- element loads otherwise
+template <typename V, int NMAX>
+__device__ __forceinline__ void load_row(const V* __restrict__ src, int nm, V (&dst)[NMAX]) {
+  if constexpr (NMAX == 8 && (sizeof(V) == 4 || sizeof(V) == 8)) {
+    if (nm == 8 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+      if constexpr (sizeof(V) == 4) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+        const float4 b = __ldg(reinterpret_cast<const float4*>(src) + 1);
+        dst[0] = a.x; dst[1] = a.y; dst[2] = a.z; dst[3] = a.w;
+        dst[4] = b.x; dst[5] = b.y; dst[6] = b.z; dst[7] = b.w;
+      } else {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const double2 a = __ldg(reinterpret_cast<const double2*>(src) + h);
+          dst[2 * h] = a.x;
+          dst[2 * h + 1] = a.y;
+        }
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < NMAX; ++m) dst[m] = m < nm ? src[m] : (V)0;
+}
+
 // one thread per covered point and XB bands; a contribution's NMAX-padded A
 // row is loaded once and reused for every band (runtime nm <= NMAX)
 template <typename T, int XB, int NMAX>
@@ -134,9 +162,11 @@ __global__ void __launch_bounds__(256) lfc_add_kernel(const LfcView l, const typ
     for (int c = l.pt_off[p]; c < c1; ++c) {
       const typename AType<T>::A* Ar = A + l.ct_aoff[c];
       const int M = l.ct_M[c], nm = l.ct_nm[c];
+      typename AType<T>::A Aw[NMAX];
+      load_row<typename AType<T>::A, NMAX>(Ar, nm, Aw);
       R Av[NMAX];
 #pragma unroll
-      for (int m = 0; m < NMAX; ++m) Av[m] = m < nm ? (R)Ar[m] : (R)0;
+      for (int m = 0; m < NMAX; ++m) Av[m] = (R)Aw[m];
       double pr = 1.0, pi = 0.0;
       if (CPLX && q >= 0) {
         const double2 ph = l.phase[(int64_t)q * l.nW + l.ct_W[c]];
@@ -147,9 +177,16 @@ __global__ void __launch_bounds__(256) lfc_add_kernel(const LfcView l, const typ
         if (i < nb) {
           const T* cx = c_xM + (x0 + i) * l.nM + M;
           T s = zero<T>();
+          if constexpr (!CPLX) {
+            T cv[NMAX];
+            load_row<T, NMAX>(cx, nm, cv);
 #pragma unroll
-          for (int m = 0; m < NMAX; ++m)
-            if (m < nm) s = fmadd(s, Av[m], cx[m]);
+            for (int m = 0; m < NMAX; ++m) s = fmadd(s, Av[m], cv[m]);
+          } else {
+#pragma unroll
+            for (int m = 0; m < NMAX; ++m)
+              if (m < nm) s = fmadd(s, Av[m], cx[m]);
+          }
           acc[i] = add(acc[i], CPLX ? phase_mul(s, pr, pi) : s);
         }
       }
@@ -196,9 +233,11 @@ __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, cons
       // real data: every image has phase 1, accumulate straight into acc
       for (int64_t r = r0 + threadIdx.x; r < r1; r += NT) {
         const int G = l.row_G[r];
+        typename AType<T>::A Aw[NM];
+        load_row<typename AType<T>::A, NM>(AW + (r - r0) * nm, nm, Aw);
         R Ar[NM];
 #pragma unroll
-        for (int m = 0; m < NM; ++m) Ar[m] = m < nm ? (R)AW[(r - r0) * nm + m] : (R)0;
+        for (int m = 0; m < NM; ++m) Ar[m] = (R)Aw[m];
 #pragma unroll
         for (int i = 0; i < XB; ++i) {
           if (x0 + i < nx) {
