@@ -381,6 +381,57 @@ def network_benchmark(args):
     print(json.dumps(out))
 
 
+def band_gemm_benchmark(args):
+    """The eigensolver's band-space GEMMs on their Si64 shape, 160 FP32 bands
+    of 56^3 = 175,616 points: the Gram matrix dv psi^T (H psi) (tensor cores,
+    three-product TF32 split, FP64-combined partial sums; plus the FP64 dots
+    that make its diagonal exact) and the rotation psi <- U psi (identity
+    split), each next to the GEMM it replaces (FP64 GEMM of widened operands;
+    FP32 SIMT GEMM).  CUDA events around `steps` calls after `warmup`.
+    Algorithmic FLOPs: 2 n^2 N per product (8.99 GFLOP); bytes: the operands
+    read once and the output written once."""
+    import torch
+    from gpaw_b200.bandops import gram_tc, rotate_tc, tf32_split
+    nb, N = 160, 56 ** 3
+    g = torch.Generator(device='cuda').manual_seed(0)
+    A = torch.randn((nb, N), generator=g, device='cuda', dtype=torch.float32)
+    B = torch.randn((nb, N), generator=g, device='cuda', dtype=torch.float32)
+    U = torch.linalg.qr(torch.eye(nb, dtype=torch.float64, device='cuda') +
+                        0.05 * torch.randn((nb, nb), generator=g, dtype=torch.float64,
+                                           device='cuda'))[0]
+    Y = torch.empty_like(A)
+    split = tf32_split(U - torch.eye(nb, dtype=torch.float64, device='cuda'))
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return 1e3 * e0.elapsed_time(e1) / args.steps
+    flop = 2.0 * nb * nb * N
+    t_gram = timed(lambda: gram_tc(A, B))
+    t_gram_d = timed(lambda: gram_tc(A, B, exact_diagonal=True))
+    t_ovl = timed(lambda: gram_tc(A, A, exact_diagonal=True))
+    t_rot = timed(lambda: rotate_tc((split[0], split[1], nb), A, out=Y, identity_split=True))
+    Uf = U.to(torch.float32)
+    out = {'workload': 'band-space GEMMs, 160 FP32 bands x 56^3 points (Si64)',
+           'gram_tc_us': round(t_gram, 1),
+           'gram_tc_exact_diagonal_us': round(t_gram_d, 1),
+           'overlap_tc_exact_diagonal_us': round(t_ovl, 1),
+           'gram_fp64_widened_us': round(timed(lambda: A.double() @ B.double().T), 1),
+           'gram_tc_TFLOPs_per_product': round(flop / t_gram / 1e6, 1),
+           'rotate_tc_identity_split_us': round(t_rot, 1),
+           'rotate_fp32_simt_gemm_us': round(timed(lambda: Uf @ A), 1),
+           'rotate_tc_GBps': round(3 * nb * N * 4 / t_rot / 1e3, 1)}
+    print(json.dumps(out))
+
+
 def cpu_reference_rate(nb_sample, threads, reps=3):
     """GPAW's own C Operator (oracle/_ref) on the host: best-of GB/s."""
     from oracle import ref, fd
@@ -465,6 +516,11 @@ def main():
                     help='time the learned preconditioner network alone: one '
                          'forward pass over 160 FP32 residuals of the 56^3 Si64 '
                          'grid per step (the command line used for ncu captures)')
+    ap.add_argument('--band-gemm-only', action='store_true',
+                    help='time the tensor-core band-space GEMMs alone on the Si64 '
+                         'shapes (160 FP32 bands x 56^3 points): Gram matrix and '
+                         'subspace rotation, next to the FP64 / SIMT GEMMs they '
+                         'replace (the command line used for ncu captures)')
     ap.add_argument('--dtype', default='f64', choices=['f64', 'f32'],
                     help='storage precision of the kernel-only run (the '
                          'benchmark line itself is FP64)')
@@ -477,6 +533,9 @@ def main():
         return
     if args.network_only:
         network_benchmark(args)
+        return
+    if args.band_gemm_only:
+        band_gemm_benchmark(args)
         return
 
     import torch

@@ -641,6 +641,7 @@ int gb_band_gram_tc(int64_t na, int64_t nb, int64_t K, const float* A, int64_t l
   if (!encode_2d(&tmA, A, (uint64_t)K, (uint64_t)na, (uint64_t)lda * 4, KB, TM) ||
       !encode_2d(&tmB, B, (uint64_t)K, (uint64_t)nb, (uint64_t)ldb * 4, KB, (uint32_t)p.NT))
     return fail(GB_E_UNSUPPORTED, "gb_band_gram_tc: cuTensorMapEncodeTiled rejected the layout");
+  cudaStream_t st = (cudaStream_t)stream;
   GramArgs g;
   g.na = (int)na;
   g.nb = (int)nb;
@@ -658,7 +659,6 @@ int gb_band_gram_tc(int64_t na, int64_t nb, int64_t K, const float* A, int64_t l
     cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT);
     attr = true;
   }
-  cudaStream_t st = (cudaStream_t)stream;
   const unsigned grid = (unsigned)(p.mtiles * p.ntiles * p.nsplit);
   gram_tc_kernel<<<grid, 384, smem, st>>>(tmA, tmB, g);
   int rc = check_launch("gram_tc_kernel");
