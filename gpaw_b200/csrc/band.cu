@@ -152,7 +152,11 @@ int gb_band_gram(int64_t nb, int k, int64_t N, const void* X, int64_t ldn, int64
                  void* stream) {
   GB_REQUIRE(nb >= 0 && N >= 0 && k >= 1 && dtype_valid(dtype), "gb_band_gram: bad arguments");
   if (nb == 0) return GB_OK;
-  GB_REQUIRE(X && out && ldi >= N && ldn >= (int64_t)k * ldi - (ldi - N), "gb_band_gram: null array or bad stride");
+  // the k vectors of every band must not overlap: band-major (each band's
+  // vectors side by side) or vector-major (each vector's bands side by side)
+  const bool band_major = ldi >= N && ldn >= (int64_t)k * ldi - (ldi - N);
+  const bool vec_major = ldn >= N && ldi >= nb * ldn - (ldn - N);
+  GB_REQUIRE(X && out && (band_major || vec_major), "gb_band_gram: null array or bad stride");
   GB_REQUIRE(nb < (int64_t)1 << 31, "gb_band_gram: too many bands");
   cudaStream_t st = (cudaStream_t)stream;
   switch (dtype) {

@@ -158,6 +158,163 @@ __global__ void __launch_bounds__(256, CC > 1 ? 2 : 3) fold_fine_kernel(const Fo
     if (j0 + q < n1) yp[(j0 + q) * n2] = acc[q];
 }
 
+// Level 0 (rh = 1, one coarse channel), marching along axis 0.  A CTA owns
+// TY full rows (j0 .. j0 + TY - 1) of one band over a chunk of planes; each
+// input plane p is staged once (cp.async, rows j0 - 1 .. j0 + TY with the
+// periodic halo columns) and every thread turns it into the three partial
+// sums S_dx(p) = sum_{dy,dz} W0[dx][dy][dz] x[p][j + dy][k + dz] of its 4
+// points, added to the output planes p - 1, p, p + 1 held in a register
+// queue: 4.5 shared loads and 27 FMAs per point for the fine part.  When
+// output plane o = p - 1 is complete, the coarse part
+// sum_e H[(o%2) - 2ex][..][..] b1[o/2 + e] is added from staged coarse
+// planes (a ring of 4; zero taps of the parity skipped) and the 4 points
+// are stored as one 16-byte vector.  Requires n2 % 4 == 0, periodic axes.
+template <int TY>
+__global__ void __launch_bounds__(256) fold0_march_kernel(const FoldArgs a, int nch) {
+  __shared__ float sW[27];
+  __shared__ float sH[216];
+  extern __shared__ __align__(16) float fm_smem[];
+  const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
+  const int m0 = n0 >> 1, m1 = n1 >> 1, m2 = n2 >> 1;
+  const int FP = n2 + 8, CP = m2 + 8;                 // staged row pitches (column c at 4 + c)
+  constexpr int FR = TY + 2, CR = TY / 2 + 2;
+  float* fslot = fm_smem;                             // [2][FR][FP]
+  float* cslot = fm_smem + 2 * FR * FP;               // [4][CR][CP]
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < 27; e += nt) sW[e] = a.F[e];
+  for (int e = tid; e < 216; e += nt) sH[e] = a.G[e];
+  const int ngx = n2 >> 2;
+  const int gx = tid % ngx, ty = tid / ngx;
+  const int j0 = blockIdx.y * TY;
+  const int j = j0 + ty, k = 4 * gx;
+  const int64_t b = blockIdx.z;
+  const int o_beg = (int)((int64_t)blockIdx.x * n0 / nch), o_end = (int)((int64_t)(blockIdx.x + 1) * n0 / nch);
+  const float* xb = a.xf + b * n0 * (int64_t)n1 * n2;
+  const float* cb = a.xc + b * (int64_t)m0 * m1 * m2;
+
+  // staging: thread (ty, gx) copies rows ty, ty + TY, ... and 16-byte
+  // chunks gx, gx + ngx, ... (no index divisions); the two halo columns of
+  // a row come from the threads gx = 0 and 1
+  auto stage_fine = [&](int p, float* dst) {
+    const float* pl = xb + (int64_t)pw(p, n0) * n1 * n2;
+    for (int r = ty; r < FR; r += TY) {
+      const float* row = pl + (int64_t)pw(j0 - 1 + r, n1) * n2;
+      float* d = dst + r * FP;
+      for (int c = gx; c < ngx; c += ngx) cp_async16(d + 4 + 4 * c, row + 4 * c);
+      if (gx == 0) cp_async4(d + 3, row + n2 - 1);                 // column -1
+      if (gx == 1 || ngx == 1) cp_async4(d + 4 + n2, row);         // column n2
+    }
+  };
+  auto stage_coarse = [&](int C, float* dst) {
+    const float* pl = cb + (int64_t)pw(C, m0) * m1 * m2;
+    for (int r = ty; r < CR; r += TY) {
+      const float* row = pl + (int64_t)pw((j0 >> 1) - 1 + r, m1) * m2;
+      float* d = dst + r * CP;
+      for (int c = gx; c < (m2 >> 1); c += ngx) cp_async8(d + 4 + 2 * c, row + 2 * c);
+      if (gx == 0) cp_async4(d + 3, row + m2 - 1);
+      if (gx == 1 || ngx == 1) cp_async4(d + 4 + m2, row);
+    }
+  };
+  auto cidx = [](int C) { return (C + 4) & 3; };
+
+  // prologue: planes o_beg - 1 and o_beg, coarse planes around o_beg / 2
+  int c_last = (o_beg >> 1) + 1;
+  stage_fine(o_beg - 1, fslot);
+  for (int C = (o_beg >> 1) - 1; C <= c_last; ++C) stage_coarse(C, cslot + cidx(C) * CR * CP);
+  cp_async_commit();
+  stage_fine(o_beg, fslot + FR * FP);
+  cp_async_commit();
+
+  float qa[4] = {0.f, 0.f, 0.f, 0.f}, qb[4] = {0.f, 0.f, 0.f, 0.f}, qc[4] = {0.f, 0.f, 0.f, 0.f};
+  const bool act = ty < TY && j < n1;
+  __syncthreads();                                  // sW, sH written
+
+  const int nsteps = o_end - o_beg + 2;
+  for (int st = 0; st < nsteps; ++st) {
+    const int p = o_beg - 1 + st;
+    cp_async_wait<1>();
+    __syncthreads();
+    if (act) {
+      const float* F = fslot + (st & 1) * FR * FP;
+      float S[3][4];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) S[d][q] = 0.f;
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy) {
+        // three 16-byte loads (scalar neighbours at a 4-float thread
+        // stride would be 4-way bank conflicts)
+        const float* rp = F + (ty + dy) * FP + 4 + k;
+        const float4 l4 = *reinterpret_cast<const float4*>(rp - 4);
+        const float4 m4 = *reinterpret_cast<const float4*>(rp);
+        const float4 r4 = *reinterpret_cast<const float4*>(rp + 4);
+        const float v[6] = {l4.w, m4.x, m4.y, m4.z, m4.w, r4.x};
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+          for (int dz = 0; dz < 3; ++dz) {
+            const float w = sW[dx * 9 + dy * 3 + dz];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) S[dx][q] = fmaf(w, v[q + dz], S[dx][q]);
+          }
+      }
+      // plane p is x[o + dx] for o = p - dx: dx = +1 -> o = p - 1, ...
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        qa[q] += S[2][q];
+        qb[q] += S[1][q];
+        qc[q] += S[0][q];
+      }
+      const int o = p - 1;
+      if (o >= o_beg) {
+        // coarse part of output plane o
+        const int px = o & 1, I0 = o >> 1, py = j & 1, K0 = k >> 1;
+#pragma unroll
+        for (int ex = -1; ex <= 1; ++ex) {
+          const int tx = px - 2 * ex + 2;
+          if (tx > 4) continue;
+          const float* Cs = cslot + cidx(I0 + ex) * CR * CP;
+#pragma unroll
+          for (int ey = -1; ey <= 1; ++ey) {
+            const int tyy = py - 2 * ey + 2;
+            if (tyy > 4) continue;
+            const float* cr = Cs + ((ty >> 1) + 1 + ey) * CP + 3 + K0;
+            const float c0 = cr[0], c1 = cr[1], c2 = cr[2], c3 = cr[3];
+            const float* g = sH + (tx * 6 + tyy) * 6;
+            const float g0 = g[0], g1 = g[1], g2 = g[2], g3 = g[3], g4 = g[4];
+            qa[0] = fmaf(g4, c0, fmaf(g2, c1, fmaf(g0, c2, qa[0])));
+            qa[1] = fmaf(g3, c1, fmaf(g1, c2, qa[1]));
+            qa[2] = fmaf(g4, c1, fmaf(g2, c2, fmaf(g0, c3, qa[2])));
+            qa[3] = fmaf(g3, c2, fmaf(g1, c3, qa[3]));
+          }
+        }
+        float* yp = a.y + ((b * n0 + o) * (int64_t)n1 + j) * n2 + k;
+        *reinterpret_cast<float4*>(yp) = make_float4(qa[0], qa[1], qa[2], qa[3]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        qa[q] = qb[q];
+        qb[q] = qc[q];
+        qc[q] = 0.f;
+      }
+    }
+    __syncthreads();
+    // refill: fine plane p + 2 into this step's slot, and the coarse plane
+    // the output completed two steps later needs
+    if (p + 2 <= o_end) {
+      stage_fine(p + 2, fslot + (st & 1) * FR * FP);
+      const int Cn = ((p + 1) >> 1) + 1;
+      if (Cn > c_last) {
+        stage_coarse(Cn, cslot + cidx(Cn) * CR * CP);
+        c_last = Cn;
+      }
+    }
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+}
+
 // r2[b][c][I] = sum_d Q[d][c] r1[b][2I + d], d in [-2, 2]^3, 16 channels
 struct StrideArgs {
   const float* x;    // (nb, n0, n1, n2) fine (level-1) grid
@@ -267,7 +424,21 @@ int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* x
              "gb_learned_fold_fine: too many grids or points per grid");
   FoldArgs a{xf, xc, y, F, G, nb, (int)n_c[0], (int)n_c[1], (int)n_c[2]};
   cudaStream_t st = (cudaStream_t)stream;
-  if (rh == 1 && cc == 1) return launch_fine(fold_fine_kernel<1, 1>, a, "fold_fine_kernel<1,1>", st);
+  if (rh == 1 && cc == 1) {
+    const int ngx = (int)(n_c[2] / 4);
+    const int TY = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
+    if (n_c[2] % 4 == 0 && n_c[1] % 2 == 0 && ngx * 2 <= 256 && n_c[1] >= TY + 2 && n_c[0] >= 2) {
+      const int nch = (int)std::min<int64_t>(n_c[0], std::max<int64_t>(1, n_c[0] / 12));
+      const size_t smem = (size_t)(2 * (TY + 2) * (n_c[2] + 8) + 4 * (TY / 2 + 2) * (n_c[2] / 2 + 8)) * sizeof(float);
+      const dim3 grid((unsigned)nch, (unsigned)((n_c[1] + TY - 1) / TY), (unsigned)nb);
+      const unsigned threads = (unsigned)(ngx * TY);
+      if (TY == 8) fold0_march_kernel<8><<<grid, threads, smem, st>>>(a, nch);
+      else if (TY == 4) fold0_march_kernel<4><<<grid, threads, smem, st>>>(a, nch);
+      else fold0_march_kernel<2><<<grid, threads, smem, st>>>(a, nch);
+      return check_launch("fold0_march_kernel");
+    }
+    return launch_fine(fold_fine_kernel<1, 1>, a, "fold_fine_kernel<1,1>", st);
+  }
   if (rh == 2 && cc == 16) return launch_fine(fold_fine_kernel<2, 16>, a, "fold_fine_kernel<2,16>", st);
   return fail(GB_E_UNSUPPORTED, "gb_learned_fold_fine: (rh, cc) not in {(1, 1), (2, 16)}");
 }

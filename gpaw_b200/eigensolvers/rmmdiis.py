@@ -49,11 +49,6 @@ class RMMDIIS(Eigensolver):
             # Re <a_n|b_n> per band, FP64 accumulation
             return wfs.band_dots(a, b) * dv
 
-        def axpy(y, a_n, x):
-            # y_n += a_n x_n for every band, in place (one launch)
-            a_n = a_n.to(torch.float64).reshape(-1)
-            band_combine(y, torch.stack([torch.ones_like(a_n), a_n], 1), [y, x])
-
         error = torch.zeros((), dtype=torch.float64, device=psit.device)
         for n1 in range(0, nb, B):
             n2 = min(n1 + B, nb)
@@ -62,18 +57,20 @@ class RMMDIIS(Eigensolver):
             Rb = R[n1:n2]
             error = error + (weights[n1:n2] * dots(Rb, Rb)).sum()
             nbl = n2 - n1
-            if self.niter > 1:
-                psit_diis = torch.empty((nbl, self.niter) + psit.shape[1:],
-                                        dtype=psit.dtype, device=psit.device)
-                R_diis = torch.empty_like(psit_diis)
-                psit_diis[:, 0] = psitb
-                R_diis[:, 0] = Rb
-            dpsit = self.preconditioner(Rb, kpt)
+            # the DIIS history: slot 0 of the wave functions is psitb itself;
+            # every later step writes its result straight into its slot (no
+            # copies), residual slots live in one slot-major array for the
+            # batched Gram kernel
+            psi_slots = [psitb]
+            R_diis = torch.empty((self.niter, nbl) + psit.shape[1:],
+                                 dtype=psit.dtype, device=psit.device)
+            R_diis[0].copy_(Rb)
+            dpsit = self.preconditioner(R_diis[0], kpt)
             dR = torch.empty_like(dpsit)
             Ht(dpsit, dR)
             P = wfs.projections(dpsit, kpt)
             self.calculate_residuals(kpt, wfs, ham, dpsit, P, eps_x, dR)
-            RdR = dots(dR, Rb)
+            RdR = dots(dR, R_diis[0])
             dRdR = dots(dR, dR)
             lam = -RdR / dRdR
             if self.limit_lambda:
@@ -83,15 +80,22 @@ class RMMDIIS(Eigensolver):
                     lam = torch.where(lam.abs() > up, up * lam.sign(), lam)
                 else:
                     lam = lam.clamp(lo, up)
-            axpy(psitb, lam, dpsit)
-            axpy(Rb, lam, dR)
+            lam2 = torch.stack([torch.ones_like(lam.reshape(-1)).to(torch.float64),
+                                lam.reshape(-1).to(torch.float64)], 1)
+            if self.niter > 1:
+                psi_slots.append(torch.empty_like(psitb))
+                band_combine(psi_slots[1], lam2, [psitb, dpsit])
+                band_combine(R_diis[1], lam2, [R_diis[0], dR])
+                cur_psi, cur_R = psi_slots[1], R_diis[1]
+            else:
+                cur_psi, cur_R = torch.empty_like(psitb), torch.empty_like(Rb)
+                band_combine(cur_psi, lam2, [psitb, dpsit])
+                band_combine(cur_R, lam2, [R_diis[0], dR])
             for nit in range(1, self.niter):
-                psit_diis[:, nit] = psitb
-                R_diis[:, nit] = Rb
                 if nit > 1 or self.limit_lambda:
                     # R_ij = <R_i|R_j> over the stored residuals (one batched
                     # Gram kernel), then the bordered DIIS system per band
-                    R_nn = wfs.band_gram(R_diis, nit + 1) * dv
+                    R_nn = wfs.band_gram(R_diis.transpose(0, 1), nit + 1) * dv
                     A = -torch.ones((nbl, nit + 2, nit + 2), dtype=torch.float64,
                                     device=psit.device)
                     A[:, :nit + 1, :nit + 1] = R_nn
@@ -99,16 +103,23 @@ class RMMDIIS(Eigensolver):
                     x = torch.zeros((nbl, nit + 2), dtype=torch.float64, device=psit.device)
                     x[:, -1] = -1.0
                     alpha = small_solve(A, x)[0][:, :-1]
-                    band_combine(psitb, alpha, [psit_diis[:, i] for i in range(nit + 1)])
-                    band_combine(Rb, alpha, [R_diis[:, i] for i in range(nit + 1)])
+                    cur_psi = torch.empty_like(psitb)
+                    cur_R = torch.empty_like(Rb)
+                    band_combine(cur_psi, alpha, psi_slots[:nit + 1])
+                    band_combine(cur_R, alpha, [R_diis[i] for i in range(nit + 1)])
                 if nit < self.niter - 1:
-                    dpsit = self.preconditioner(Rb, kpt)
-                    axpy(psitb, lam, dpsit)
-                    Ht(psitb, Rb)
-                    P = wfs.projections(psitb, kpt)
-                    self.calculate_residuals(kpt, wfs, ham, psitb, P, eps_x, Rb)
-            dpsit = self.preconditioner(Rb, kpt)
+                    dpsit = self.preconditioner(cur_R, kpt)
+                    nxt = torch.empty_like(psitb)
+                    band_combine(nxt, lam2, [cur_psi, dpsit])
+                    psi_slots.append(nxt)
+                    Ht(nxt, R_diis[nit + 1])
+                    P = wfs.projections(nxt, kpt)
+                    self.calculate_residuals(kpt, wfs, ham, nxt, P, eps_x, R_diis[nit + 1])
+                    cur_psi, cur_R = nxt, R_diis[nit + 1]
+            dpsit = self.preconditioner(cur_R, kpt)
             step = (torch.full_like(lam, self.trial_step) if self.trial_step is not None
                     else lam)
-            axpy(psitb, step, dpsit)
+            step2 = torch.stack([torch.ones_like(step.reshape(-1)).to(torch.float64),
+                                 step.reshape(-1).to(torch.float64)], 1)
+            band_combine(psitb, step2, [cur_psi, dpsit])
         return error

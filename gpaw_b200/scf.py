@@ -486,11 +486,12 @@ class _GraphedIteration:
     def _capture_b(self, calc, wfs, kpt, es, weights):
         es.subspace_rotate(wfs, kpt, self.eps, self.V, self.Htpsit)
         err = es.update_bands(calc, wfs, kpt, weights)
-        wfs.orthonormalize(kpt)
+        wfs.orthonormalize(kpt, out=self.psit)
         E = calc.total_energy(kpt) * Hartree
         ddens = calc.update_density()
         calc.update_hamiltonian()
-        self.psit.copy_(kpt.psit_nG)
+        if kpt.psit_nG.data_ptr() != self.psit.data_ptr():
+            self.psit.copy_(kpt.psit_nG)
         if self.P is not None:
             self.P.copy_(kpt.P_nM)
         self.out = torch.stack([E, err, ddens, calc._judge_flag()])

@@ -91,7 +91,11 @@ class FDWaveFunctions:
         B = b_nG.reshape(b_nG.shape[0], -1).to(wide)
         return (A.conj() @ B.T) * self.gd.dv
 
-    def orthonormalize(self, kpt):
+    def orthonormalize(self, kpt, out=None):
+        """psi <- L^-1 psi with S = L L^H (gpaw/wavefunctions/fdpw.py:
+        394-424); `out` (optional, not aliasing psi) receives the result and
+        becomes kpt.psit_nG -- a captured SCF step writes into its static
+        buffer this way instead of copying."""
         psit = kpt.psit_nG
         S = self.matrix(psit, psit).to(torch.complex128 if self.dtype.is_complex
                                          else torch.float64)
@@ -101,11 +105,13 @@ class FDWaveFunctions:
             L, torch.eye(L.shape[0], dtype=L.dtype, device=L.device), upper=False)
         # psi_n <- sum_m Linv[n, m]^* psi_m  (S = L L^H, <phi|phi> = 1)
         nb = psit.shape[0]
-        y = (rotate_tc(Linv, psit, identity_split=True)
+        y = (rotate_tc(Linv, psit, out=out, identity_split=True)
              if psit.dtype == torch.float32 else None)
         if y is None:
             C = Linv.conj().to(self.dtype)
             y = (C @ psit.reshape(nb, -1)).reshape(psit.shape)
+            if out is not None:
+                y = out.copy_(y)
         kpt.psit_nG = y
         kpt.P_nM = self.projections(kpt.psit_nG, kpt)
 

@@ -254,7 +254,7 @@ int gb_learned_fold_stride(const float* x, const float* Q, float* y, int64_t nb,
  * FP64 accumulation for every storage dtype (no dv factor):
  *   dots: out[n] = Re sum_G conj(a[n*lda + G]) b[n*ldb + G], G < N
  *   gram: out[n][i][j] = Re sum_G conj(X[n*ldn + i*ldi + G]) X[n*ldn + j*ldi + G],
- *         i, j < k <= 5
+ *         i, j < k <= 5 (band-major or vector-major strides, no overlap)
  * ==================================================================== */
 int gb_band_dots(int64_t nb, int64_t N, const void* a, int64_t lda,
                  const void* b, int64_t ldb, int dtype, double* out,
