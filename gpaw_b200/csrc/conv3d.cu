@@ -228,6 +228,117 @@ __global__ void __launch_bounds__(ConvTile<COUT, CZT>::THREADS) conv3d_fwd_kerne
   }
 }
 
+// 16 -> 16 channels on a periodic grid small enough to stage a few whole
+// planes (the level-2 convolution of the learned preconditioner): a CTA
+// takes TP output planes of one band, stages input planes z0 - 1 .. z0 + TP
+// of all 16 channels with their periodic halo ([plane][ci][n1 + 2][n2 + 2])
+// and the weights ([ci][tap][co]) once, then every thread accumulates two
+// neighbouring points of a row x 16 output channels: per (input channel,
+// tap) two shared loads of the input, four broadcast 16-byte weight loads
+// and 32 FMAs.
+constexpr int C16_TP = 2;
+
+__global__ void __launch_bounds__(256) conv16_periodic_kernel(const ConvArgs a) {
+  extern __shared__ __align__(16) float c16_smem[];
+  const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
+  const int P1 = n1 + 2, P2 = n2 + 2, PP = P1 * P2;
+  float* sw = c16_smem;                       // [16][27][16]
+  float* sx = c16_smem + 16 * 27 * 16;        // [TP + 2][16][P1][P2]
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < 16 * 16 * 27; e += nt) {
+    const int co = e / (16 * 27), ci = (e / 27) % 16, k = e % 27;
+    sw[(ci * 27 + k) * 16 + co] = __bfloat162float(a.w[e]);
+  }
+  const int z0 = blockIdx.x * C16_TP;
+  const int64_t b = blockIdx.y;
+  const int64_t n012 = (int64_t)n0 * n1 * n2;
+  const float* xb = a.x + b * 16 * n012;
+  // stage (TP + 2) planes x 16 channels with the periodic halo
+  const int nst = (C16_TP + 2) * 16 * PP;
+  for (int e = tid; e < nst; e += nt) {
+    const int px = e % P2;
+    int r = e / P2;
+    const int py = r % P1;
+    r /= P1;
+    const int ci = r % 16, pz = r / 16;
+    int z = z0 - 1 + pz, y = py - 1, x = px - 1;
+    z = z < 0 ? z + n0 : (z >= n0 ? z - n0 : z);
+    y = y < 0 ? y + n1 : (y >= n1 ? y - n1 : y);
+    x = x < 0 ? x + n2 : (x >= n2 ? x - n2 : x);
+    sx[e] = __ldg(xb + ci * n012 + ((int64_t)z * n1 + y) * n2 + x);
+  }
+  __syncthreads();
+  const int hx = n2 >> 1;                      // point pairs per row
+  const int per_plane = n1 * hx;
+  const int zl = tid / per_plane;
+  if (zl >= C16_TP || z0 + zl >= n0) return;
+  const int rem = tid % per_plane;
+  const int y = rem / hx, x = 2 * (rem % hx);
+  float acc0[16], acc1[16];
+#pragma unroll
+  for (int co = 0; co < 16; ++co) { acc0[co] = 0.f; acc1[co] = 0.f; }
+#pragma unroll 1
+  for (int ci = 0; ci < 16; ++ci) {
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy) {
+        const float* row = sx + ((zl + dz) * 16 + ci) * PP + (y + dy) * P2 + x;
+        const float v0 = row[0], v1 = row[1], v2 = row[2], v3 = row[3];
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+          const float va = dx == 0 ? v0 : (dx == 1 ? v1 : v2);
+          const float vb = dx == 0 ? v1 : (dx == 1 ? v2 : v3);
+          const float4* w4 = reinterpret_cast<const float4*>(sw + (ci * 27 + dz * 9 + dy * 3 + dx) * 16);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const float4 w = w4[q];
+            acc0[4 * q] = fmaf(w.x, va, acc0[4 * q]);
+            acc0[4 * q + 1] = fmaf(w.y, va, acc0[4 * q + 1]);
+            acc0[4 * q + 2] = fmaf(w.z, va, acc0[4 * q + 2]);
+            acc0[4 * q + 3] = fmaf(w.w, va, acc0[4 * q + 3]);
+            acc1[4 * q] = fmaf(w.x, vb, acc1[4 * q]);
+            acc1[4 * q + 1] = fmaf(w.y, vb, acc1[4 * q + 1]);
+            acc1[4 * q + 2] = fmaf(w.z, vb, acc1[4 * q + 2]);
+            acc1[4 * q + 3] = fmaf(w.w, vb, acc1[4 * q + 3]);
+          }
+        }
+      }
+  }
+  float* yb = a.y + b * 16 * n012 + ((int64_t)(z0 + zl) * n1 + y) * n2 + x;
+#pragma unroll
+  for (int co = 0; co < 16; ++co) {
+    float* yp = yb + co * n012;
+    if (a.accumulate) {
+      yp[0] += acc0[co];
+      yp[1] += acc1[co];
+    } else {
+      yp[0] = acc0[co];
+      yp[1] = acc1[co];
+    }
+  }
+}
+
+// smem bytes of conv16_periodic_kernel for a grid (0 when it does not apply)
+static size_t conv16_smem(const ConvArgs& a) {
+  if (!(a.pbc0 && a.pbc1 && a.pbc2) || a.n2 % 2 || a.n0 < 2) return 0;
+  if ((int64_t)C16_TP * a.n1 * (a.n2 / 2) > 256 || a.nb > 65535) return 0;
+  const size_t bytes = (size_t)(16 * 27 * 16 + (C16_TP + 2) * 16 * (a.n1 + 2) * (a.n2 + 2)) * sizeof(float);
+  return bytes <= 200 * 1024 ? bytes : 0;
+}
+
+static int conv16_launch(const ConvArgs& a, size_t smem, cudaStream_t st) {
+  static size_t attr = 0;
+  if (smem > attr) {
+    cudaFuncSetAttribute(conv16_periodic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = smem;
+  }
+  const int threads = ((C16_TP * a.n1 * (a.n2 / 2) + 31) / 32) * 32;
+  const dim3 grid((unsigned)((a.n0 + C16_TP - 1) / C16_TP), (unsigned)a.nb);
+  conv16_periodic_kernel<<<grid, threads, smem, st>>>(a);
+  return check_launch("conv16_periodic_kernel");
+}
+
 // dw[co][ci][k] += sum_b sum_p dy[b][co][p] x[b][ci][p + o_k]   (FP32)
 // grid: (cin * cout channel pairs) x (chunks of the band x point range);
 // each CTA reduces its chunk and adds its 27 sums to dw with atomics
@@ -313,7 +424,11 @@ int gb_conv3d_forward(const float* x, const void* w_bf16, float* y, int64_t nb, 
   cudaStream_t st = (cudaStream_t)stream;
   if (cin == 1 && cout == 1) return fwd_launch<1, 1>(a, st);
   if (cin == 1 && cout == 16) return fwd_launch<1, 16>(a, st);
-  if (cin == 16 && cout == 16) return fwd_launch<16, 16>(a, st);
+  if (cin == 16 && cout == 16) {
+    const size_t sm16 = conv16_smem(a);
+    if (sm16) return conv16_launch(a, sm16, st);
+    return fwd_launch<16, 16>(a, st);
+  }
   if (cin == 16 && cout == 1) return fwd_launch<16, 1>(a, st);
   return fail(GB_E_UNSUPPORTED, "gb_conv3d_forward: channel pair not in {(1,1), (1,16), (16,16), (16,1)}");
 }

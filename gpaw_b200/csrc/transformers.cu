@@ -531,11 +531,259 @@ static int restrict_cfg(const gb_transformer* t, const void* in, void* out, int6
   return launch_persistent<C>(restrict_kernel<C>, a, total, st, 4 + K);
 }
 
+// k = 2 restriction of real data on a grid periodic on every axis (the
+// preconditioner's and the learned network's first transfer), marching
+// along axis 0: a CTA owns TYC coarse rows of one band over a chunk of
+// coarse planes; each fine plane it needs (rows 2 J0 - 1 .. 2 J0 + 2 TYC - 1
+// plus the wrap-around columns) is staged once with cp.async into a two-slot
+// ring, every thread restricts it in-plane for two neighbouring coarse
+// points (axis 2, then axis 1: the general kernel's arithmetic, in its
+// order) and the axis-0 step takes the last three fine planes from a
+// register queue.  Rows must be 16-byte aligned.
+template <typename T, int TYC>
+__global__ void __launch_bounds__(256) restrict2_march_kernel(const TrArgs a, int nch) {
+  extern __shared__ __align__(16) unsigned char r2m_smem[];
+  T* slot = reinterpret_cast<T*>(r2m_smem);
+  constexpr int VEC = 16 / (int)sizeof(T);
+  const int nf0 = a.ni[0], nf1 = a.ni[1], nf2 = a.ni[2];
+  const int nc0 = a.no[0], nc1 = a.no[1], nc2 = a.no[2];
+  const int FR = 2 * TYC + 1, FP = nf2 + 2 * VEC + 8;   // fine column c at VEC + c
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int ngx = (nc2 + 1) >> 1;
+  const int gx = tid % ngx, ty = tid / ngx;
+  const int J0 = blockIdx.y * TYC, J = J0 + ty, K0 = 2 * gx;
+  const int64_t b = blockIdx.z;
+  const int I_beg = (int)((int64_t)blockIdx.x * nc0 / nch), I_end = (int)((int64_t)(blockIdx.x + 1) * nc0 / nch);
+  const T* src = reinterpret_cast<const T*>(a.in) + b * (int64_t)nf0 * nf1 * nf2;
+  T* dst = reinterpret_cast<T*>(a.out) + b * (int64_t)nc0 * nc1 * nc2;
+  const T w0 = (T)a.w[0], half = (T)0.5, alpha = (T)a.alpha;
+  const int r0 = 2 * J0 + a.off[1] - 1;                 // first staged fine row
+  auto wrap = [](int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); };
+  auto stage = [&](int p, T* d) {
+    const T* pl = src + (int64_t)wrap(p, nf0) * nf1 * nf2;
+    const int chunks = nf2 / VEC;
+    for (int e = tid; e < FR * (chunks + 2); e += nt) {
+      const int r = e / (chunks + 2), c = e % (chunks + 2);
+      const T* row = pl + (int64_t)wrap(r0 + r, nf1) * nf2;
+      T* dr = d + r * FP;
+      if (c < chunks) cp_async16(dr + VEC + c * VEC, row + c * VEC);
+      else if (c == chunks) cp_async_elem(dr + VEC - 1, row + nf2 - 1);   // column -1
+      else cp_async_elem(dr + VEC + nf2, row);                          // column nf2
+    }
+  };
+  const int p_beg = 2 * I_beg + a.off[0] - 1, p_end = 2 * (I_end - 1) + a.off[0] + 1;
+  stage(p_beg, slot);
+  cp_async_commit();
+  T q0[2] = {0, 0}, q1[2] = {0, 0}, q2[2] = {0, 0};
+  const bool act = ty < TYC && J < nc1;
+  for (int p = p_beg; p <= p_end; ++p) {
+    const int s = (p - p_beg) & 1;
+    if (p + 1 <= p_end) stage(p + 1, slot + (s ^ 1) * FR * FP);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    if (act) {
+      const T* P = slot + s * FR * FP + 2 * ty * FP + VEC + 2 * K0 + a.off[2];
+      T g[3][2];
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy) {
+        const T* f = P + dy * FP;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          g[dy][h] = half * fmadd(f[2 * h], w0, add(f[2 * h + 1], f[2 * h - 1]));
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        q0[h] = q1[h];
+        q1[h] = q2[h];
+        q2[h] = half * fmadd(g[1][h], w0, add(g[2][h], g[0][h]));
+      }
+      const int tI = p - a.off[0] - 1;                  // fine plane 2I + off + 1 just arrived
+      if (tI >= 2 * I_beg && (tI & 1) == 0) {
+        const int I = tI >> 1;
+        T* o = dst + ((int64_t)I * nc1 + J) * nc2 + K0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (K0 + h < nc2) o[h] = alpha * (half * fmadd(q1[h], w0, add(q2[h], q0[h])));
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+}
+
+template <typename T>
+static int restrict2_march_launch(const gb_transformer* t, const void* in, void* out, int64_t nin,
+                                  cudaStream_t st, double alpha) {
+  constexpr int VEC = 16 / (int)sizeof(T);
+  TrArgs a;
+  fill_common(t, a, nullptr);
+  a.in = in; a.out = out; a.nbatch = nin; a.alpha = alpha;
+  const int ngx = (a.no[2] + 1) / 2;
+  const int TYC = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
+  const int nch = std::max(1, std::min(a.no[0], a.no[0] / 8));
+  const size_t smem = (size_t)2 * (2 * TYC + 1) * (a.ni[2] + 2 * VEC + 8) * sizeof(T);
+  const dim3 grid((unsigned)nch, (unsigned)((a.no[1] + TYC - 1) / TYC), (unsigned)nin);
+  const unsigned threads = (unsigned)(ngx * TYC);
+  if (TYC == 8) restrict2_march_kernel<T, 8><<<grid, threads, smem, st>>>(a, nch);
+  else if (TYC == 4) restrict2_march_kernel<T, 4><<<grid, threads, smem, st>>>(a, nch);
+  else restrict2_march_kernel<T, 2><<<grid, threads, smem, st>>>(a, nch);
+  return check_launch("restrict2_march_kernel");
+}
+
+template <typename T>
+static bool restrict2_march_ok(const gb_transformer* t, int64_t nin, const double* ph) {
+  if (!t->pbc[0] || !t->pbc[1] || !t->pbc[2] || nin > 65535 || nin < 1) return false;
+  if (ph)
+    for (int i = 0; i < 12; ++i)
+      if (ph[i] != ((i % 2) ? 0.0 : 1.0)) return false;
+  const int64_t nf2 = t->nin_c[2];
+  const int64_t ngx = (t->nout_c[2] + 1) / 2;
+  const int64_t tyc = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
+  // single-wrap periodic indices: at least 2 * TYC fine rows, 2 planes
+  return (nf2 * (int64_t)sizeof(T)) % 16 == 0 && ngx * 2 <= 256 && t->nin_c[0] >= 2 &&
+         t->nin_c[1] >= 2 * tyc && nf2 >= 2 * (16 / (int)sizeof(T)) && t->nout_c[1] >= 1;
+}
+
+// k = 2 interpolation of real data on a grid periodic on every axis (fine
+// point 2C on coarse point C), marching along axis 0 over coarse planes: a
+// CTA owns TYF fine rows of one band over a chunk of coarse planes; each
+// coarse plane (rows F0/2 .. F0/2 + TYF/2 plus the wrap-around column) is
+// staged once into a two-slot ring; every thread interpolates it for four
+// neighbouring fine columns of its row (axis 2, then axis 1: the general
+// kernel's arithmetic, in its order) and, once coarse plane C + 1 is in,
+// writes fine planes 2C and 2C + 1 with the alpha / gamma * y epilogue as
+// 16-byte vectors.  Rows must be 16-byte aligned.
+template <typename T, int TYF>
+__global__ void __launch_bounds__(256) interp2_march_kernel(const TrArgs a, int nch) {
+  extern __shared__ __align__(16) unsigned char i2m_smem[];
+  T* slot = reinterpret_cast<T*>(i2m_smem);
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int CRR = TYF / 2 + 1;
+  const int nc0 = a.ni[0], nc1 = a.ni[1], nc2 = a.ni[2];
+  const int nf1 = a.no[1], nf2 = a.no[2];
+  const int CP = nc2 + 2 * VEC + 8;                    // coarse column c at VEC + c
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int ngx = nf2 >> 2;
+  const int gx = tid % ngx, ty = tid / ngx;
+  const int F0 = blockIdx.y * TYF, F = F0 + ty, k = 4 * gx;
+  const int64_t b = blockIdx.z;
+  const int C_beg = (int)((int64_t)blockIdx.x * nc0 / nch), C_end = (int)((int64_t)(blockIdx.x + 1) * nc0 / nch);
+  const T* src = reinterpret_cast<const T*>(a.in) + b * (int64_t)nc0 * nc1 * nc2;
+  const int64_t fplane = (int64_t)nf1 * nf2;
+  T* dst = reinterpret_cast<T*>(a.out) + b * 2 * (int64_t)nc0 * fplane;
+  const T* ysrc = a.y ? reinterpret_cast<const T*>(a.y) + b * 2 * (int64_t)nc0 * fplane : nullptr;
+  const T w0 = (T)a.w[0], alpha = (T)a.alpha, gamma = (T)a.gamma;
+  auto wrap = [](int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); };
+  auto stage = [&](int g, T* d) {
+    const T* pl = src + (int64_t)wrap(g, nc0) * nc1 * nc2;
+    const int chunks = nc2 / VEC;
+    for (int e = tid; e < CRR * (chunks + 1); e += nt) {
+      const int r = e / (chunks + 1), c = e % (chunks + 1);
+      const T* row = pl + (int64_t)wrap((F0 >> 1) + r, nc1) * nc2;
+      T* dr = d + r * CP;
+      if (c < chunks) cp_async16(dr + VEC + c * VEC, row + c * VEC);
+      else cp_async_elem(dr + VEC + nc2, row);                 // column nc2
+    }
+  };
+  stage(C_beg, slot);
+  cp_async_commit();
+  T qp[4];                                             // u of the previous coarse plane
+  const bool act = ty < TYF && F < nf1;
+  for (int g = C_beg; g <= C_end; ++g) {
+    const int s = (g - C_beg) & 1;
+    if (g + 1 <= C_end) stage(g + 1, slot + (s ^ 1) * CRR * CP);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    if (act) {
+      const T* P = slot + s * CRR * CP + VEC + (k >> 1);
+      const int rl = (F >> 1) - (F0 >> 1);
+      T A[2][4];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const T* row = P + (rl + h) * CP;
+        const T c0 = row[0], c1 = row[1], c2 = row[2];
+        A[h][0] = c0;
+        A[h][1] = w0 * add(c0, c1);
+        A[h][2] = c1;
+        A[h][3] = w0 * add(c1, c2);
+      }
+      T u[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) u[q] = (F & 1) ? w0 * add(A[0][q], A[1][q]) : A[0][q];
+      if (g > C_beg) {
+        const int C = g - 1;
+#pragma unroll
+        for (int par = 0; par < 2; ++par) {
+          const int64_t o = (int64_t)(2 * C + par) * fplane + (int64_t)F * nf2 + k;
+          T x[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            T v = par == 0 ? qp[q] : w0 * add(qp[q], u[q]);
+            v = alpha * v;
+            if (ysrc) v = fmadd(v, gamma, ysrc[o + q]);
+            x[q] = v;
+          }
+          if constexpr (sizeof(T) == 4) {
+            *reinterpret_cast<float4*>(dst + o) = make_float4(x[0], x[1], x[2], x[3]);
+          } else {
+            reinterpret_cast<double2*>(dst + o)[0] = make_double2(x[0], x[1]);
+            reinterpret_cast<double2*>(dst + o)[1] = make_double2(x[2], x[3]);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) qp[q] = u[q];
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+}
+
+template <typename T>
+static bool interp2_march_ok(const gb_transformer* t, int64_t nin, const double* ph, const void* y) {
+  if (!t->pbc[0] || !t->pbc[1] || !t->pbc[2] || nin > 65535 || nin < 1) return false;
+  if (ph)
+    for (int i = 0; i < 12; ++i)
+      if (ph[i] != ((i % 2) ? 0.0 : 1.0)) return false;
+  for (int c = 0; c < 3; ++c)
+    if (t->skip0[c] != 0 || t->cbeg[c] != 0 || t->nout_c[c] != 2 * t->nin_c[c]) return false;
+  const int64_t nc2 = t->nin_c[2], nf2 = t->nout_c[2];
+  const int64_t ngx = nf2 / 4;
+  const int64_t tyf = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
+  (void)y;
+  return (nc2 * (int64_t)sizeof(T)) % 16 == 0 && nf2 % 4 == 0 && ngx * 2 <= 256 && t->nin_c[0] >= 1 &&
+         t->nin_c[1] >= tyf / 2 + 1 && nc2 >= 16 / (int)sizeof(T);
+}
+
+template <typename T>
+static int interp2_march_launch(const gb_transformer* t, const void* in, void* out, int64_t nin,
+                                cudaStream_t st, double alpha, const void* y, double gamma) {
+  constexpr int VEC = 16 / (int)sizeof(T);
+  TrArgs a;
+  fill_common(t, a, nullptr);
+  a.in = in; a.out = out; a.nbatch = nin; a.alpha = alpha; a.y = y; a.gamma = gamma;
+  const int ngx = a.no[2] / 4;
+  const int TYF = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
+  const int nch = std::max(1, std::min(a.ni[0], a.ni[0] / 7));
+  const size_t smem = (size_t)2 * (TYF / 2 + 1) * (a.ni[2] + 2 * VEC + 8) * sizeof(T);
+  const dim3 grid((unsigned)nch, (unsigned)((a.no[1] + TYF - 1) / TYF), (unsigned)nin);
+  const unsigned threads = (unsigned)(ngx * TYF);
+  if (TYF == 8) interp2_march_kernel<T, 8><<<grid, threads, smem, st>>>(a, nch);
+  else if (TYF == 4) interp2_march_kernel<T, 4><<<grid, threads, smem, st>>>(a, nch);
+  else interp2_march_kernel<T, 2><<<grid, threads, smem, st>>>(a, nch);
+  return check_launch("interp2_march_kernel");
+}
+
 // coarse rows of at most 16 points (the coarse levels of small grids) use a
 // 16 x 16 tile, wider ones 8 x 32: no more than half a warp idles on a row
 template <typename T, int K>
 static int restrict_k(const gb_transformer* t, const void* in, void* out, int64_t nin,
                       const double* ph, cudaStream_t st, double alpha) {
+  if constexpr (K == 2 && !Elem<T>::cplx) {
+    if (restrict2_march_ok<T>(t, nin, ph)) return restrict2_march_launch<T>(t, in, out, nin, st, alpha);
+  }
   if (t->nout_c[2] <= 16) return restrict_cfg<T, K, 16, 16>(t, in, out, nin, ph, st, alpha);
   return restrict_cfg<T, K, 8, 32>(t, in, out, nin, ph, st, alpha);
 }
@@ -543,6 +791,9 @@ static int restrict_k(const gb_transformer* t, const void* in, void* out, int64_
 template <typename T, int K>
 static int interpolate_k(const gb_transformer* t, const void* in, void* out, int64_t nin,
                          const double* ph, cudaStream_t st, double alpha, const void* y, double gamma) {
+  if constexpr (K == 2 && !Elem<T>::cplx) {
+    if (interp2_march_ok<T>(t, nin, ph, y)) return interp2_march_launch<T>(t, in, out, nin, st, alpha, y, gamma);
+  }
   constexpr int RZ = sizeof(T) == 4 ? 4 : (sizeof(T) == 8 ? 2 : 1);
   using C = ICfg<T, K, 16, 32, 2, RZ, 2>;
   TrArgs a;

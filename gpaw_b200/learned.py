@@ -493,20 +493,26 @@ class LearnedPreconditioner:
     (scaled by the multigrid step of this grid), with the multigrid as judge
     and fallback.
 
-    Every call also applies the multigrid to `nprobe` bands and compares; a
-    relative deviation above `tolerance` (or a non-finite output) sets the
-    device flag `failed`.  Nothing is read back during the call, so it runs
+    Every `probe_every`-th call (default 3: once per RMM-DIIS pass) also
+    applies the multigrid to `nprobe` bands and compares; a relative
+    deviation above `tolerance` (or a non-finite output) sets the device
+    flag `failed`.  Nothing is read back during the call, so it runs
     inside a captured SCF step; the SCF driver reads the flag once per
     iteration with its other scalars and, when it is set, continues with the
     multigrid alone (`fallback`)."""
 
-    def __init__(self, net: ConvNet, multigrid, tolerance=0.5, nprobe=2):
+    def __init__(self, net: ConvNet, multigrid, tolerance=0.5, nprobe=2, probe_every=3):
         self.net = net
         self.multigrid = multigrid
         self.fallback = multigrid
         self.step = multigrid.step
         self.tolerance = tolerance
         self.nprobe = nprobe
+        # judge one call in `probe_every` (3 = once per RMM-DIIS pass with its
+        # default niter = 3 preconditioner calls); a captured SCF step holds
+        # the same calls on every replay, so the cadence is fixed
+        self.probe_every = max(1, int(probe_every))
+        self._calls = 0
         self.failed = torch.zeros((), dtype=torch.bool, device=net.device)
         self.deviation = torch.zeros((), dtype=torch.float64, device=net.device)
         # periodic grids (sizes divisible by 4): the folded inference form
@@ -522,6 +528,7 @@ class LearnedPreconditioner:
         self(R)
         self.failed.zero_()
         self.deviation.zero_()
+        self._calls = 0
 
     def __call__(self, R, kpt=None, ekin=None, out=None):
         if R.ndim == 3:
@@ -529,13 +536,16 @@ class LearnedPreconditioner:
             return self(R[None], kpt, out=o)[0]
         y = (self.folded.forward(R) if self.folded is not None
              else self.net.forward(R, scale=self.step))
-        k = min(self.nprobe, R.shape[0])
-        probe = self.multigrid(R[:k].contiguous(), kpt).to(torch.float32)
-        dev = self.net.relative_error_from(y[:k], probe).max().to(torch.float64)
+        probe_now = self._calls % self.probe_every == 0
+        self._calls += 1
+        if probe_now:
+            k = min(self.nprobe, R.shape[0])
+            probe = self.multigrid(R[:k].contiguous(), kpt).to(torch.float32)
+            dev = self.net.relative_error_from(y[:k], probe).max().to(torch.float64)
+            self.deviation.copy_(torch.maximum(self.deviation, dev))
+            bad = ~torch.isfinite(dev) | (dev > self.tolerance)
+            self.failed.logical_or_(bad)
         y = y.to(R.dtype)
-        self.deviation.copy_(torch.maximum(self.deviation, dev))
-        bad = ~torch.isfinite(dev) | (dev > self.tolerance)
-        self.failed.logical_or_(bad)
         if out is not None:
             out.copy_(y)
             return out

@@ -437,6 +437,19 @@ def h2(vacuum=3.0, d=0.74):
     return ['H', 'H'], pos, cell
 
 
+_POOL = None
+
+
+def _graph_pool():
+    """One private memory pool for every captured SCF step of the process:
+    the blocks a released graph gave back are there for the next capture,
+    which then allocates (almost) nothing new."""
+    global _POOL
+    if _POOL is None:
+        _POOL = torch.cuda.graph_pool_handle()
+    return _POOL
+
+
 class _GraphedIteration:
     """One SCF iteration as two CUDA graphs around the subspace eigensolver.
 
@@ -462,7 +475,7 @@ class _GraphedIteration:
         wide = torch.complex128 if wfs.dtype.is_complex else torch.float64
         self.eps = torch.empty(nb, dtype=torch.float64, device=self.psit.device)
         self.V = torch.empty((nb, nb), dtype=wide, device=self.psit.device)
-        self.pool = torch.cuda.graph_pool_handle()
+        self.pool = _graph_pool()
         # capture on a side stream with capture_begin/capture_end (the
         # torch.cuda.graph context manager would also run gc.collect() and
         # empty the allocator's cache, whose re-filling costs far more than
