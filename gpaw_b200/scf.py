@@ -438,15 +438,28 @@ def h2(vacuum=3.0, d=0.74):
 
 
 _POOL = None
+_POOL_KEEPER = None
 
 
 def _graph_pool():
     """One private memory pool for every captured SCF step of the process:
     the blocks a released graph gave back are there for the next capture,
-    which then allocates (almost) nothing new."""
-    global _POOL
+    which then allocates (almost) nothing new.  torch retires a pool once no
+    graph uses it, so a one-op graph captured into it at creation stays
+    alive for the process and keeps the pool."""
+    global _POOL, _POOL_KEEPER
     if _POOL is None:
-        _POOL = torch.cuda.graph_pool_handle()
+        pool = torch.cuda.graph_pool_handle()
+        x = torch.zeros(1, device='cuda')
+        keep = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            keep.capture_begin(pool=pool)
+            x.add_(1.0)
+            keep.capture_end()
+        torch.cuda.current_stream().wait_stream(side)
+        _POOL, _POOL_KEEPER = pool, (keep, x)
     return _POOL
 
 
