@@ -26,6 +26,10 @@
 
 namespace gb {
 
+// tcgen05 implicit-GEMM convolution of 16 input channels (conv_tc.cu)
+int conv16_tc_try(const float* x, const void* w_bf16, float* y, int64_t nb, int cout, int n0, int n1, int n2,
+                  int accumulate, cudaStream_t st, int* launched);
+
 struct ConvArgs {
   const float* x;
   const float* x2;          // when set: input channel 1 comes from here (CIN = 2)
@@ -425,6 +429,12 @@ int gb_conv3d_forward(const float* x, const void* w_bf16, float* y, int64_t nb, 
   if (cin == 1 && cout == 1) return fwd_launch<1, 1>(a, st);
   if (cin == 1 && cout == 16) return fwd_launch<1, 16>(a, st);
   if (cin == 16 && cout == 16) {
+    // tensor cores first (periodic grids), then the staged-plane kernel
+    if (a.pbc0 && a.pbc1 && a.pbc2) {
+      int launched = 0;
+      const int rc = conv16_tc_try(x, w_bf16, y, nb, 16, a.n0, a.n1, a.n2, accumulate, st, &launched);
+      if (rc != GB_OK || launched) return rc;
+    }
     const size_t sm16 = conv16_smem(a);
     if (sm16) return conv16_launch(a, sm16, st);
     return fwd_launch<16, 16>(a, st);

@@ -673,6 +673,8 @@ int gb_device_errors(int clear, int* code) {
   *code = gb::device_error_flag(clear);
   const int tc = gb::band_tc_error_flag(clear);
   if (!*code) *code = tc;
+  const int ctc = gb::conv_tc_error_flag(clear);
+  if (!*code) *code = ctc;
   return GB_OK;
 }
 

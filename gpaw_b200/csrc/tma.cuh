@@ -71,6 +71,7 @@ __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
 // device-side error flag (set by timed-out waits); read with gb_device_errors()
 int device_error_flag(int clear);
 int band_tc_error_flag(int clear);   // the tensor-core band GEMMs' flag
+int conv_tc_error_flag(int clear);   // the tensor-core convolution's flag
 __device__ void raise_device_error(int code);
 
 // host: encode a 4-D tiled tensor map (dims innermost first, strides in bytes)
