@@ -25,6 +25,7 @@ exchange step on one grid per band batch), value = total bytes / max time.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import re
@@ -292,6 +293,9 @@ def scf_benchmark(train_steps=400):
         w = si64(prec, block)
         w.run(maxiter=8, energy_tol=0.0, graph=graph)
         del w
+        # a calculation holds reference cycles: collect it now, so that its
+        # device buffers (and the graph pool's blocks) are free for the next
+        gc.collect()
     t0 = time.perf_counter()
     c = si64('fp32')
     R, T = collect_pairs(c, iterations=6, per_call=8, max_pairs=400)
@@ -304,6 +308,7 @@ def scf_benchmark(train_steps=400):
     err1 = float(net.relative_error_t(R[-32:], T[-32:]).mean())
     t_prep = time.perf_counter() - t0
     del c
+    gc.collect()
     out = {'workload': 'Si64 diamond (2x2x2 cells, a=10.86 A, sigma=0.05 A), h=0.2 A '
                        '(56^3), 160 bands, LDA, Gamma; SCF to 1e-5 eV/electron',
            'training': {'pairs': int(len(R)), 'steps': train_steps,
@@ -336,6 +341,7 @@ def scf_benchmark(train_steps=400):
             r['max_occupied_eigenvalue_error_eV'] = float(np.abs(eps - ref[1]).max())
         out[name] = r
         del c
+        gc.collect()
     a = out['fp64_multigrid_plain']
     for name in ('fp32_learned_batched', 'fp32_multigrid_batched', 'fp64_multigrid_batched'):
         b = out[name]

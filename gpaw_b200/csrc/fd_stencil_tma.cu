@@ -128,6 +128,26 @@ __device__ __forceinline__ void ldv(const T* p, T (&v)[N]) {
   }
 }
 
+// N consecutive elements from global memory: 16-byte loads when N elements
+// make whole 16-byte chunks (the caller guarantees the alignment), else
+// element loads
+template <typename V, int N>
+__device__ __forceinline__ void ldg_run(const V* __restrict__ p, V (&v)[N]) {
+  if constexpr ((N * sizeof(V)) % 16 == 0) {
+    constexpr int E = 16 / (int)sizeof(V);
+#pragma unroll
+    for (int h = 0; h < N / E; ++h) {
+      const float4 x = __ldg(reinterpret_cast<const float4*>(p) + h);
+      const V* e = reinterpret_cast<const V*>(&x);
+#pragma unroll
+      for (int k = 0; k < E; ++k) v[h * E + k] = e[k];
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < N; ++c) v[c] = p[c];
+  }
+}
+
 template <typename T, int H, int R1, int R2, int VB>
 __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                         const __grid_constant__ CUtensorMap tmH,
@@ -354,11 +374,17 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
               if (yrow + r >= n1) continue;
               const int64_t p = pbase + (int64_t)r * n2;
               if (epi) {
+                // y and the potential: 16-byte loads of this thread's R2
+                // points (p is a multiple of R2, both bases 16-byte aligned)
+                T yv[R2];
+                R vv[R2];
+                if (ybase) ldg_run<T, R2>(ybase + p, yv);
+                if (vpot) ldg_run<R, R2>(vpot + p, vv);
 #pragma unroll
                 for (int c = 0; c < R2; ++c) {
                   T v = fmadd(scale((R)a.alpha, acc[r][c]), (R)a.beta, q[cu][r][c]);
-                  if (ybase) v = fmadd(v, (R)a.gamma, ybase[p + c]);
-                  if (vpot) v = fmadd(v, vpot[p + c], q[cu][r][c]);
+                  if (ybase) v = fmadd(v, (R)a.gamma, yv[c]);
+                  if (vpot) v = fmadd(v, vv[c], q[cu][r][c]);
                   acc[r][c] = v;
                 }
               }
@@ -622,6 +648,7 @@ int star_tma_apply(const gb_operator* op, const void* in, void* out, int64_t nin
   }
   if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) { g_tma_reason = "unaligned data"; return 1; }
   if (ep.y && (reinterpret_cast<uintptr_t>(ep.y) & 15)) { g_tma_reason = "unaligned y"; return 1; }
+  if (ep.vpot && (reinterpret_cast<uintptr_t>(ep.vpot) & 15)) { g_tma_reason = "unaligned potential"; return 1; }
   if (op->n[0] < op->H || op->n[1] < op->H || op->n[2] < 8) { g_tma_reason = "grid shorter than the stencil"; return 1; }
   switch (dtype) {
     case GB_DTYPE_F64:

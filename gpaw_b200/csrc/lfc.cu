@@ -54,6 +54,13 @@ struct gb_lfc {
   int* row_G = nullptr;       // [rows] grid point of every global row
   int64_t* vol_aoff = nullptr;  // [nW] offset (doubles) of row0 in A
   std::vector<int> h_gr_nm;
+  // all-band add for real data (every volume has <= 16 functions): A rows
+  // zero-padded to fast_nmax, in contribution order
+  int fast_nmax = 0;          // 8 or 16; 0 = not built
+  bool full32 = false;        // every contribution: nm == fast_nmax, M and nM multiples of 4
+  bool full64 = false;        // the same with multiples of 2 (16-byte FP64 loads)
+  float* Ac32 = nullptr;      // [C][fast_nmax]
+  double* Ac64 = nullptr;
   std::vector<void*> allocations;
 };
 
@@ -302,6 +309,147 @@ __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, cons
   }
 }
 
+// ------------------------------------------------ real data, all bands
+// For real data (Gamma point: every periodic image has phase 1) and at most
+// 16 functions per volume, the add runs every band in one pass: one thread
+// per covered point holds the zero-padded A rows of its first KREG
+// contributions in registers (a copy of A in contribution order, so a warp's
+// row loads are contiguous) and loops over the bands XU at a time, issuing
+// the XU read-modify-write loads of a[x][G] before the coefficient loads and
+// FMAs of those bands.  Per band it sums the contributions in point order,
+// m within each, as lfc_add_kernel does, so the two give identical results.
+// (The same all-band treatment of the integrate, with row tiles of A staged in
+// shared memory per (group, 16-band) CTA, measured no faster than
+// lfc_integrate_kernel on the Si64 shape and slower in FP64, so the integrate
+// keeps the kernel above.)
+template <typename T, int NMAX, bool FULL>
+__device__ __forceinline__ void load_coef(const T* __restrict__ cx, int nm, T (&v)[NMAX]) {
+  if constexpr (FULL) {
+    // every contribution has NMAX functions at a 16-byte aligned offset
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+      for (int h = 0; h < NMAX / 4; ++h) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(cx) + h);
+        v[4 * h] = a.x; v[4 * h + 1] = a.y; v[4 * h + 2] = a.z; v[4 * h + 3] = a.w;
+      }
+    } else {
+#pragma unroll
+      for (int h = 0; h < NMAX / 2; ++h) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(cx) + h);
+        v[2 * h] = a.x; v[2 * h + 1] = a.y;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < NMAX; ++m) v[m] = m < nm ? __ldg(cx + m) : (T)0;
+  }
+}
+
+template <typename T, int NMAX>
+__device__ __forceinline__ void load_padded_row(const T* __restrict__ src, T (&v)[NMAX]) {
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int h = 0; h < NMAX / 4; ++h) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(src) + h);
+      v[4 * h] = a.x; v[4 * h + 1] = a.y; v[4 * h + 2] = a.z; v[4 * h + 3] = a.w;
+    }
+  } else {
+#pragma unroll
+    for (int h = 0; h < NMAX / 2; ++h) {
+      const double2 a = __ldg(reinterpret_cast<const double2*>(src) + h);
+      v[2 * h] = a.x; v[2 * h + 1] = a.y;
+    }
+  }
+}
+
+// acc[u] += sum_m A[m] c[x0 + u][M + m], u < NU, cx = &c[x0][M] (the
+// contribution's sum is formed first, then added, as in lfc_add_kernel)
+template <typename T, int NMAX, bool FULL, int NU>
+__device__ __forceinline__ void add_contribution(const T (&A)[NMAX], const T* __restrict__ cx, int nM, int nm,
+                                                 T (&acc)[NU]) {
+#pragma unroll
+  for (int u = 0; u < NU; ++u) {
+    T cv[NMAX];
+    load_coef<T, NMAX, FULL>(cx, nm, cv);
+    T t = (T)0;
+#pragma unroll
+    for (int m = 0; m < NMAX; ++m) t = fmadd(t, A[m], cv[m]);
+    acc[u] += t;
+    cx += nM;
+  }
+}
+
+// bands x0 .. x0+NU-1 of one point: a[x][G] += sum_k sum_m A_k[m] c[x][M_k + m]
+template <typename T, int NMAX, int KREG, bool FULL, int NU>
+__device__ __forceinline__ void add_point_bands(const T (&A)[KREG][NMAX], const T* const (&cb)[KREG],
+                                                const int (&nmk)[KREG], int K, int k0,
+                                                const int* __restrict__ ct_M, const int* __restrict__ ct_nm,
+                                                const T* __restrict__ Ac, const T* __restrict__ c_xM, int nM,
+                                                int64_t x0, T* __restrict__ ax, int64_t nG) {
+  // the read-modify-write loads first: their latency overlaps the FMAs
+  T av[NU], acc[NU];
+  {
+    const T* q = ax;
+#pragma unroll
+    for (int u = 0; u < NU; ++u) {
+      av[u] = *q;
+      acc[u] = (T)0;
+      q += nG;
+    }
+  }
+  const int64_t xo = x0 * nM;
+#pragma unroll
+  for (int k = 0; k < KREG; ++k)
+    if (k < K) add_contribution<T, NMAX, FULL, NU>(A[k], cb[k] + xo, nM, nmk[k], acc);
+  for (int k = KREG; k < K; ++k) {
+    T Ak[NMAX];
+    load_padded_row<T, NMAX>(Ac + (int64_t)(k0 + k) * NMAX, Ak);
+    add_contribution<T, NMAX, FULL, NU>(Ak, c_xM + ct_M[k0 + k] + xo, nM, ct_nm[k0 + k], acc);
+  }
+  T* q = ax;
+#pragma unroll
+  for (int u = 0; u < NU; ++u) {
+    *q = av[u] + acc[u];
+    q += nG;
+  }
+}
+
+template <typename T, int NMAX, int KREG, bool FULL, int XU>
+__global__ void __launch_bounds__(256) lfc_add_bands_kernel(const int* __restrict__ pt_G,
+                                                            const int* __restrict__ pt_off,
+                                                            const int* __restrict__ ct_M,
+                                                            const int* __restrict__ ct_nm,
+                                                            const T* __restrict__ Ac, int64_t P,
+                                                            const T* __restrict__ c_xM, int nM,
+                                                            T* __restrict__ a_xG, int64_t nG, int64_t nx) {
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const int G = pt_G[p];
+  const int k0 = pt_off[p], K = pt_off[p + 1] - k0;
+  T A[KREG][NMAX];
+  const T* cb[KREG];
+  int nmk[KREG];
+#pragma unroll
+  for (int k = 0; k < KREG; ++k) {
+    if (k < K) {
+      load_padded_row<T, NMAX>(Ac + (int64_t)(k0 + k) * NMAX, A[k]);
+      cb[k] = c_xM + ct_M[k0 + k];
+      nmk[k] = ct_nm[k0 + k];
+    } else {
+#pragma unroll
+      for (int m = 0; m < NMAX; ++m) A[k][m] = (T)0;
+      cb[k] = c_xM;
+      nmk[k] = 0;
+    }
+  }
+  const int64_t nfull = nx / XU * XU;
+  T* ax = a_xG + G;
+  for (int64_t x0 = 0; x0 < nfull; x0 += XU, ax += XU * nG)
+    add_point_bands<T, NMAX, KREG, FULL, XU>(A, cb, nmk, K, k0, ct_M, ct_nm, Ac, c_xM, nM, x0, ax, nG);
+  for (int64_t x0 = nfull; x0 < nx; ++x0, ax += nG)
+    add_point_bands<T, NMAX, KREG, FULL, 1>(A, cb, nmk, K, k0, ct_M, ct_nm, Ac, c_xM, nM, x0, ax, nG);
+}
+
 template <typename T, int NM>
 static int integrate_nm(const gb_lfc* l, int gbeg, int gcount, const void* a, void* c, int64_t nx, int q,
                         cudaStream_t st) {
@@ -321,6 +469,28 @@ static int nm_class(int nm) {
   for (int c : {1, 2, 4, 8, 16, 32, 64})
     if (nm <= c) return c;
   return 0;
+}
+
+template <typename T>
+static int add_fast(const gb_lfc* l, const void* c, void* a, int64_t nx, cudaStream_t st) {
+  const T* Ac;
+  if constexpr (sizeof(T) == 4) Ac = l->Ac32; else Ac = l->Ac64;
+  const bool full = (sizeof(T) == 4 ? l->full32 : l->full64) && (reinterpret_cast<uintptr_t>(c) & 15) == 0;
+  constexpr int NT = 256, XU = 8;
+  const unsigned grid = (unsigned)((l->P + NT - 1) / NT);
+  const T* cc = (const T*)c;
+  T* aa = (T*)a;
+#define GB_ADD_BANDS(NMAX, KREG, FULL)                                                                        \
+  lfc_add_bands_kernel<T, NMAX, KREG, FULL, XU><<<grid, NT, 0, st>>>(l->pt_G, l->pt_off, l->ct_M, l->ct_nm, Ac, \
+                                                                      l->P, cc, l->nM, aa, l->nG, nx)
+  constexpr int K8 = sizeof(T) == 4 ? 4 : 2, K16 = sizeof(T) == 4 ? 2 : 1;
+  if (l->fast_nmax == 8) {
+    if (full) GB_ADD_BANDS(8, K8, true); else GB_ADD_BANDS(8, K8, false);
+  } else {
+    if (full) GB_ADD_BANDS(16, K16, true); else GB_ADD_BANDS(16, K16, false);
+  }
+#undef GB_ADD_BANDS
+  return check_launch("lfc_add_bands_kernel");
 }
 
 template <typename T>
@@ -362,6 +532,9 @@ static int add_nm(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cu
 template <typename T>
 static int add_t(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st) {
   if (l->P == 0) return GB_OK;
+  if constexpr (!Elem<T>::cplx) {
+    if (l->fast_nmax) return add_fast<T>(l, c, a, nx, st);
+  }
   switch (nm_class(l->maxnm)) {
     case 1: return add_nm<T, 8, 1>(l, c, a, nx, q, st);
     case 2: return add_nm<T, 8, 2>(l, c, a, nx, q, st);
@@ -484,6 +657,21 @@ int gb_lfc_new(int nW, const double* A_all, const int64_t* ngm_W, const int* nm_
     for (int W : kv.second) gv_W.push_back(W);
     gr_voff.push_back((int)gv_W.size());
   }
+  // zero-padded A rows in contribution order for the all-band real add
+  std::vector<double> hAc;
+  if (l->maxnm <= 16) {
+    const int F = l->maxnm <= 8 ? 8 : 16;
+    l->fast_nmax = F;
+    bool full32 = nM % 4 == 0, full64 = nM % 2 == 0;
+    hAc.assign(ct_aoff.size() * F, 0.0);
+    for (size_t c = 0; c < ct_aoff.size(); ++c) {
+      for (int m = 0; m < ct_nm[c]; ++m) hAc[c * F + m] = A_all[ct_aoff[c] + m];
+      full32 = full32 && ct_nm[c] == F && ct_M[c] % 4 == 0;
+      full64 = full64 && ct_nm[c] == F && ct_M[c] % 2 == 0;
+    }
+    l->full32 = full32;
+    l->full64 = full64;
+  }
   l->ngroups = (int)gr_M.size();
   l->h_gr_nm = gr_nm;
   l->P = (int64_t)pt_G.size();
@@ -505,6 +693,18 @@ int gb_lfc_new(int nW, const double* A_all, const int64_t* ngm_W, const int* nm_
     ok = l->A32 != nullptr;
     if (ok && l->nA) {
       to_float<<<std::min<int64_t>((l->nA + 255) / 256, 4096), 256>>>(l->A64, l->A32, l->nA);
+      ok = cudaDeviceSynchronize() == cudaSuccess;
+    }
+  }
+  if (ok && l->fast_nmax) {
+    ok = upload(l, &l->Ac64, hAc);
+    if (ok) {
+      l->Ac32 = dalloc<float>(l, hAc.size());
+      ok = l->Ac32 != nullptr;
+    }
+    if (ok && !hAc.empty()) {
+      to_float<<<std::min<int64_t>(((int64_t)hAc.size() + 255) / 256, 4096), 256>>>(l->Ac64, l->Ac32,
+                                                                                      (int64_t)hAc.size());
       ok = cudaDeviceSynchronize() == cudaSuccess;
     }
   }

@@ -217,3 +217,68 @@ def test_microbench_full_size_adjoint():
     perm = torch.randperm(nx, device='cuda')
     cM2 = lfc.integrate(a[perm].contiguous(), {})
     assert torch.equal(cM2, cM[perm])
+
+
+def _dense_lfc(nfun, natoms=12, n=24, rc_ang=2.2, seed=5):
+    """natoms atoms with nfun functions each (l = 0, 1 radial functions
+    up to nfun) in a small periodic box, cutoffs large enough that a point
+    lies in up to ~natoms spheres."""
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.lfc import LFC
+    from gpaw_b200.spline import Spline
+    bohr = 0.52917721
+    rc = rc_ang / bohr
+    r = np.linspace(0, rc, 61)
+    ls = {1: [0], 4: [0, 1], 8: [0, 1, 0, 1], 9: [0, 1, 0, 1, 0], 12: [0, 1, 0, 1, 0, 1]}[nfun]
+    spl = [(l, rc, np.exp(-(r / (0.9 / bohr))**2) * (1 + 0.3 * j)) for j, l in enumerate(ls)]
+    L = n * 0.2 / bohr
+    gd = GridDescriptor((n, n, n), (L, L, L), True)
+    spos = np.random.default_rng(seed).random((natoms, 3))
+    lfc = LFC(gd, [[Spline.from_data(*s) for s in spl]] * natoms)
+    lfc.set_positions(spos)
+    return gd, lfc, spos, spl
+
+
+@pytest.mark.parametrize('nfun', [1, 4, 8, 9, 12])
+def test_add_all_bands_vs_oracle(nfun):
+    """The all-band real add (contributions held in registers, the rest
+    re-read; full 16-byte coefficient rows or element loads; a band tail)
+    against the oracle's dense sum in FP64, FP32 within 1e-5 of it, and an
+    unaligned coefficient array (element loads) equal to the aligned one."""
+    gd, lfc, spos, spl = _dense_lfc(nfun)
+    Phi = ol.dense_functions(gd.N_c, gd.cell_cv, gd.pbc_c, spos, [spl] * len(spos))
+    assert lfc.Mmax == nfun * len(spos)
+    rng = np.random.default_rng(11)
+    nx = 11
+    c = rng.standard_normal((nx, lfc.Mmax))
+    a0 = rng.standard_normal((nx,) + tuple(gd.n_c))
+    want = ol.add(a0.copy(), c, Phi)
+    b = torch.from_numpy(a0).cuda()
+    lfc.add_M(b, torch.from_numpy(c).cuda())
+    assert rel(b.cpu().numpy(), want) < 1e-12
+    b32 = torch.from_numpy(a0).cuda().float()
+    lfc.add_M(b32, torch.from_numpy(c).cuda().float())
+    assert rel(b32.double().cpu().numpy(), want) < 1e-5
+    # the same coefficients at an address 4 bytes past a 16-byte boundary
+    buf = torch.zeros(nx * lfc.Mmax + 1, dtype=torch.float32, device='cuda')
+    cu = buf[1:].view(nx, lfc.Mmax)
+    cu.copy_(torch.from_numpy(c))
+    b32u = torch.from_numpy(a0).cuda().float()
+    lfc.add_M(b32u, cu)
+    assert torch.equal(b32u, b32)
+
+
+def test_add_all_bands_equals_band_blocks():
+    """Adding all bands at once equals adding them in blocks of 10 (the
+    reference's RMM-DIIS block size), bit for bit."""
+    gd, lfc, spos, spl = _dense_lfc(8)
+    g = torch.Generator(device='cuda').manual_seed(2)
+    nx = 37
+    c = torch.randn((nx, lfc.Mmax), generator=g, device='cuda', dtype=torch.float32)
+    a0 = torch.randn((nx,) + tuple(gd.n_c), generator=g, device='cuda', dtype=torch.float32)
+    b = a0.clone()
+    lfc.add_M(b, c)
+    b2 = a0.clone()
+    for x in range(0, nx, 10):
+        lfc.add_M(b2[x:x + 10], c[x:x + 10].contiguous())
+    assert torch.equal(b, b2)
