@@ -517,6 +517,90 @@ static int launch_star(const gb_operator* op, const void* in, void* out, int64_t
   return check_launch("star_kernel");
 }
 
+// Small real grids (the coarsest multigrid level, 14^3 for a 56^3 grid):
+// the tiles of star_kernel would leave most threads idle and march a few
+// planes per CTA through its staging pipeline, so one thread per point reads
+// its 6H neighbours straight from global memory (the grid stays in L1/L2).
+// Same terms in the same order as star_kernel (axis 0, axis 2, axis 1, m
+// ascending; the FP32 difference form), so both give identical results.
+template <typename T, int H>
+__global__ void __launch_bounds__(256) star_direct_kernel(const StarArgs args) {
+  constexpr bool DIFF = sizeof(T) == 4;
+  const int n0 = args.n0, n1 = args.n1, n2 = args.n2;
+  const int64_t n12 = (int64_t)n1 * n2, n012 = n12 * n0;
+  const int64_t total = args.nbatch * n012;
+  const bool epi = args.alpha != 1.0 || args.beta != 0.0 || args.y != nullptr || args.vpot != nullptr;
+  const T* __restrict__ vpot = reinterpret_cast<const T*>(args.vpot);
+  const T c0 = DIFF ? (T)args.c0diff : (T)args.c0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t band = e / n012;
+    const int64_t g = e - band * n012;
+    const int i0 = (int)(g / n12);
+    const int i1 = (int)((g - (int64_t)i0 * n12) / n2);
+    const int i2 = (int)(g - (int64_t)i0 * n12 - (int64_t)i1 * n2);
+    const T* __restrict__ src = reinterpret_cast<const T*>(args.in) + band * n012;
+    const T xc = src[g];
+    T x = scale(c0, xc);
+    // axis 0
+#pragma unroll
+    for (int m = 0; m <= 2 * H; ++m) {
+      if (m == H) continue;
+      int j = i0 + m - H;
+      T v = (T)0;
+      if (j >= 0 && j < n0) v = src[g + (int64_t)(m - H) * n12];
+      else if (args.pbc0) v = src[(int64_t)wrap_index(j, n0) * n12 + (g - (int64_t)i0 * n12)];
+      x = fmadd(x, (T)args.a[0][m - H + HMAX], DIFF ? v - xc : v);
+    }
+    // axis 2
+#pragma unroll
+    for (int m = 0; m <= 2 * H; ++m) {
+      if (m == H) continue;
+      int j = i2 + m - H;
+      T v = (T)0;
+      if (j >= 0 && j < n2) v = src[g + (m - H)];
+      else if (args.pbc2) v = src[g - i2 + wrap_index(j, n2)];
+      x = fmadd(x, (T)args.a[2][m - H + HMAX], DIFF ? v - xc : v);
+    }
+    // axis 1
+#pragma unroll
+    for (int m = 0; m <= 2 * H; ++m) {
+      if (m == H) continue;
+      int j = i1 + m - H;
+      T v = (T)0;
+      if (j >= 0 && j < n1) v = src[g + (int64_t)(m - H) * n2];
+      else if (args.pbc1) v = src[g + (int64_t)(wrap_index(j, n1) - i1) * n2];
+      x = fmadd(x, (T)args.a[1][m - H + HMAX], DIFF ? v - xc : v);
+    }
+    if (epi) {
+      T v = fmadd(scale((T)args.alpha, x), (T)args.beta, xc);
+      if (args.y) v = fmadd(v, (T)args.gamma, reinterpret_cast<const T*>(args.y)[e]);
+      if (vpot) v = fmadd(v, vpot[g], xc);
+      x = v;
+    }
+    reinterpret_cast<T*>(args.out)[e] = x;
+  }
+}
+
+template <typename T, int H>
+static int launch_star_direct(const gb_operator* op, const void* in, void* out, int64_t nin,
+                              cudaStream_t stream, const Epilogue& ep) {
+  StarArgs a{};
+  a.in = in; a.out = out; a.nbatch = nin;
+  a.n0 = (int)op->n[0]; a.n1 = (int)op->n[1]; a.n2 = (int)op->n[2];
+  a.pbc0 = op->pbc[0]; a.pbc1 = op->pbc[1]; a.pbc2 = op->pbc[2];
+  a.c0 = op->center;
+  a.c0diff = op->center;
+  for (int c = 0; c < 3; ++c)
+    for (int m = 0; m < 2 * HMAX + 1; ++m) a.c0diff += op->a[c][m];
+  memcpy(a.a, op->a, sizeof(a.a));
+  a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma; a.y = ep.y; a.vpot = ep.vpot;
+  const int64_t total = nin * op->n[0] * op->n[1] * op->n[2];
+  const int64_t blocks = std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 8);
+  star_direct_kernel<T, H><<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, stream>>>(a);
+  return check_launch("star_direct_kernel");
+}
+
 // Per-element-size tile shapes.  (R1 x R2) points per thread, (TY x TZ)
 // threads; R2 * sizeof(T) = 16 bytes so row windows are single LDS.128s and a
 // warp's 16 lanes along axis 2 read 256 contiguous bytes (no bank conflicts).
@@ -530,6 +614,19 @@ template <int H> struct StarTile<double2, H> { using C = StarCfg<double2, H, (H 
 template <typename T>
 static int dispatch_star(const gb_operator* op, const void* in, void* out, int64_t nin,
                          const double* ph, cudaStream_t st, const Epilogue& ep) {
+  if constexpr (!Elem<T>::cplx) {
+    // tiles of star_kernel less than a quarter used: one thread per point
+    using C1 = typename StarTile<T, 1>::C;
+    const int64_t n1 = op->n[1], n2 = op->n[2];
+    const int64_t tiled = (int64_t)ceil_div((int)n1, C1::T1) * C1::T1 * ceil_div((int)n2, C1::T2) * C1::T2;
+    if (op->H <= 3 && 4 * n1 * n2 < tiled) {
+      switch (op->H) {
+        case 1: return launch_star_direct<T, 1>(op, in, out, nin, st, ep);
+        case 2: return launch_star_direct<T, 2>(op, in, out, nin, st, ep);
+        default: return launch_star_direct<T, 3>(op, in, out, nin, st, ep);
+      }
+    }
+  }
   switch (op->H) {
     case 1: return launch_star<typename StarTile<T, 1>::C>(op, in, out, nin, ph, st, ep);
     case 2: return launch_star<typename StarTile<T, 2>::C>(op, in, out, nin, ph, st, ep);

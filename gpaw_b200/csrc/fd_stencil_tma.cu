@@ -374,18 +374,30 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
               if (yrow + r >= n1) continue;
               const int64_t p = pbase + (int64_t)r * n2;
               if (epi) {
-                // y and the potential: 16-byte loads of this thread's R2
-                // points (p is a multiple of R2, both bases 16-byte aligned)
-                T yv[R2];
-                R vv[R2];
-                if (ybase) ldg_run<T, R2>(ybase + p, yv);
-                if (vpot) ldg_run<R, R2>(vpot + p, vv);
+                if constexpr (sizeof(T) == 4) {
+                  // FP32: y and the potential as 16-byte loads of this
+                  // thread's R2 points (p is a multiple of R2, both bases
+                  // 16-byte aligned); the FP64 kernels run faster, epilogue
+                  // or not, with the element loads below
+                  T yv[R2];
+                  R vv[R2];
+                  if (ybase) ldg_run<T, R2>(ybase + p, yv);
+                  if (vpot) ldg_run<R, R2>(vpot + p, vv);
 #pragma unroll
-                for (int c = 0; c < R2; ++c) {
-                  T v = fmadd(scale((R)a.alpha, acc[r][c]), (R)a.beta, q[cu][r][c]);
-                  if (ybase) v = fmadd(v, (R)a.gamma, yv[c]);
-                  if (vpot) v = fmadd(v, vv[c], q[cu][r][c]);
-                  acc[r][c] = v;
+                  for (int c = 0; c < R2; ++c) {
+                    T v = fmadd(scale((R)a.alpha, acc[r][c]), (R)a.beta, q[cu][r][c]);
+                    if (ybase) v = fmadd(v, (R)a.gamma, yv[c]);
+                    if (vpot) v = fmadd(v, vv[c], q[cu][r][c]);
+                    acc[r][c] = v;
+                  }
+                } else {
+#pragma unroll
+                  for (int c = 0; c < R2; ++c) {
+                    T v = fmadd(scale((R)a.alpha, acc[r][c]), (R)a.beta, q[cu][r][c]);
+                    if (ybase) v = fmadd(v, (R)a.gamma, ybase[p + c]);
+                    if (vpot) v = fmadd(v, vpot[p + c], q[cu][r][c]);
+                    acc[r][c] = v;
+                  }
                 }
               }
 #pragma unroll

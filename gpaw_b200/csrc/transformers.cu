@@ -513,7 +513,11 @@ static int launch_persistent(KernelT kernel, const TrArgs& a, int64_t total, cud
     if (occ < 1) occ = 1;
   }
   int64_t blocks = (int64_t)sm_count() * occ;
-  blocks = std::min<int64_t>(blocks, std::max<int64_t>(1, total / min_steps));
+  // at least min_steps planes per CTA amortise its (2K-1)-plane prologue --
+  // unless that would leave SMs idle (one small grid, e.g. the density's
+  // 112^3 -> 56^3): then the prologue's L2 re-reads cost less than idle SMs
+  const int64_t by_steps = total / min_steps;
+  blocks = std::min<int64_t>(blocks, by_steps >= sm_count() ? by_steps : std::max<int64_t>(1, total));
   kernel<<<(unsigned)blocks, C::NT, C::SMEM, st>>>(a);
   return check_launch("transformer kernel");
 }
