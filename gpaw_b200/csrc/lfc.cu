@@ -238,6 +238,10 @@ __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, cons
     }
     if constexpr (!CPLX) {
       // real data: every image has phase 1, accumulate straight into acc
+      // FP32: four rows per pass put 16 gathered loads in flight (1.1x on
+      // the Si64 shape); FP64 measured no faster unrolled
+      constexpr int RUN = sizeof(R) == 4 ? 4 : 1;
+#pragma unroll RUN
       for (int64_t r = r0 + threadIdx.x; r < r1; r += NT) {
         const int G = l.row_G[r];
         typename AType<T>::A Aw[NM];
