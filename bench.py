@@ -351,6 +351,43 @@ def scf_benchmark(train_steps=400):
     return out
 
 
+def lfc_benchmark(args):
+    """The projector LFC of the Si64 SCF on its production shape: 64 Si
+    atoms (2 s + 2 p radial functions merged into 8 functions per atom), the
+    56^3 periodic grid, 160 FP32 bands.  CUDA events around `steps` calls of
+    the add (a += sum_a p^a c^a, the nonlocal term of the residuals) and of
+    the integrate (the projections <p^a|psi>) after `warmup` untimed ones.
+    Algorithmic bytes: the add reads and writes, the integrate reads, every
+    covered point of every band once."""
+    import torch
+    from gpaw_b200.scf import Calculation, si_diamond
+    sym, pos, cell = si_diamond(2, 5.43, rattle=0.05, seed=0)
+    c = Calculation(sym, pos, cell, True, h=0.2, nbands=160, xc='LDA', precision='fp32')
+    pt = c.wfs.pt
+    n_c = tuple(c.gd.n_c)
+    g = torch.Generator(device='cuda').manual_seed(0)
+    a = torch.randn((160,) + n_c, generator=g, device='cuda', dtype=torch.float32)
+    b = torch.randn((160,) + n_c, generator=g, device='cuda', dtype=torch.float32)
+    cM = torch.randn((160, pt.Mmax), generator=g, device='cuda', dtype=torch.float32)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps * 1e3
+    t_add = timed(lambda: pt.add_M(b, cM))
+    t_int = timed(lambda: pt.integrate(a, {}))
+    print(json.dumps({'workload': 'Si64 projector LFC, 160 x 56^3 FP32 bands, 64 atoms x 8 functions',
+                      'add_us': round(t_add, 1), 'integrate_us': round(t_int, 1)}))
+
+
 def network_benchmark(args):
     """The learned preconditioner's forward pass on its production shape:
     160 FP32 residuals of the 56^3 periodic Si64 grid (h = 0.194 A), the
@@ -525,6 +562,10 @@ def main():
                     help='time the learned preconditioner network alone: one '
                          'forward pass over 160 FP32 residuals of the 56^3 Si64 '
                          'grid per step (the command line used for ncu captures)')
+    ap.add_argument('--lfc-only', action='store_true',
+                    help='time the projector LFC add and integrate alone on the '
+                         'Si64 shape (64 atoms x 8 functions, 160 FP32 bands of '
+                         '56^3; the command line used for ncu captures)')
     ap.add_argument('--band-gemm-only', action='store_true',
                     help='time the tensor-core band-space GEMMs alone on the Si64 '
                          'shapes (160 FP32 bands x 56^3 points): Gram matrix and '
@@ -542,6 +583,9 @@ def main():
         return
     if args.network_only:
         network_benchmark(args)
+        return
+    if args.lfc_only:
+        lfc_benchmark(args)
         return
     if args.band_gemm_only:
         band_gemm_benchmark(args)
