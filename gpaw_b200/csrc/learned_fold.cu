@@ -23,7 +23,12 @@
 // network to delta inputs, so they inherit its BF16 weights and transfer
 // coefficients exactly.
 //
-// Both kernels read their neighbourhoods through L1 (__ldg) with the lanes
+// Level 1 runs as two launches: fold_fine_kernel<2, 0> writes the 5^3 fine
+// part, then fold_parity16_kernel adds the 16-channel coarse part as a
+// parity convolution (one thread per coarse point, all 8 fine points of its
+// parity block from one load of each channel's 27 neighbours).
+//
+// The kernels read their neighbourhoods through L1 (__ldg) with the lanes
 // of a warp along a grid row (coalesced), keep the weights in shared memory
 // and give every thread a column of 4 output rows (fold_fine: each loaded
 // input row serves all of them) or two neighbouring coarse points with all
@@ -62,10 +67,11 @@ __global__ void __launch_bounds__(256, CC > 1 ? 2 : 3) fold_fine_kernel(const Fo
   constexpr int FW = 2 * RH + 1;
   constexpr int NR = JB + 2 * RH;          // input rows per plane
   __shared__ float sF[FW * FW * FW];
-  __shared__ float sG[CC * 216];
+  __shared__ float sG[CC > 0 ? CC * 216 : 1];
   const int tid = threadIdx.y * 32 + threadIdx.x;
   for (int e = tid; e < FW * FW * FW; e += 256) sF[e] = a.F[e];
-  for (int e = tid; e < CC * 216; e += 256) sG[e] = a.G[e];
+  if constexpr (CC > 0)
+    for (int e = tid; e < CC * 216; e += 256) sG[e] = a.G[e];
   __syncthreads();
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
   const int m0 = n0 >> 1, m1 = n1 >> 1, m2 = n2 >> 1;
@@ -108,6 +114,7 @@ __global__ void __launch_bounds__(256, CC > 1 ? 2 : 3) fold_fine_kernel(const Fo
   // coarse part: coarse rows j0/2 - 1 .. j0/2 + JB/2, columns k/2 - 1 .. k/2 + 1;
   // the weights one (channel, plane offset) needs -- 5 row parities x 3
   // column offsets for this thread's column parity -- go to registers once
+  if constexpr (CC > 0) {
   const int I0 = i >> 1, J0 = j0 >> 1, K0 = k >> 1;
   const int px = i & 1, pz = k & 1;
   int kc[3];
@@ -151,6 +158,7 @@ __global__ void __launch_bounds__(256, CC > 1 ? 2 : 3) fold_fine_kernel(const Fo
         }
       }
     }
+  }
   }
   float* yp = a.y + b * n0 * (int64_t)plane + i * plane + k;
 #pragma unroll
@@ -388,6 +396,102 @@ __global__ void __launch_bounds__(256) fold_stride_kernel(const StrideArgs a) {
   }
 }
 
+// The 16-channel coarse part of level 1 as a parity convolution:
+//   y[2J + par] += sum_c sum_e G[c][par - 2e + 2] a2[c][J + e],
+// par in {0,1}^3, e in {-1,0,1}^3 (tap t = par - 2e + 2 per axis; t = 5, an
+// odd parity with e = -1, is zero).  One thread per coarse point J loads the
+// 27 neighbours of a channel once and feeds all 8 fine points of its parity
+// block: 125 FMAs per 27 loads, against one output per gathered
+// neighbourhood in fold_fine_kernel.  A CTA owns one coarse plane of one band;
+// every CTA stages G reordered into the order the unrolled loops consume it
+// (channel, parity, tap), 128 floats per channel, so each 16-byte broadcast
+// shared load serves four FMAs.
+constexpr int NPAR = 125;   // (3 + 2)^3 taps over the 8 parities
+
+__device__ __forceinline__ constexpr int par_taps(int p) { return p ? 2 : 3; }
+// e of the j-th tap of parity p: p = 0 -> -1, 0, 1; p = 1 -> 0, 1
+__device__ __forceinline__ constexpr int par_e(int p, int j) { return p ? j : j - 1; }
+
+__global__ void __launch_bounds__(256) fold_parity16_kernel(const FoldArgs a) {
+  __shared__ __align__(16) float sW[16 * 128];
+  const int tid = threadIdx.x;
+  // reorder G[c][tx][ty][tz] (t in 0..5) into (c, parity, tap) order
+  for (int e = tid; e < 16 * 128; e += blockDim.x) {
+    const int c = e >> 7, k = e & 127;
+    float w = 0.f;
+    if (k < NPAR) {
+      int kk = k, par = 0;
+      for (; par < 8; ++par) {
+        const int n = par_taps(par >> 2) * par_taps((par >> 1) & 1) * par_taps(par & 1);
+        if (kk < n) break;
+        kk -= n;
+      }
+      const int px = par >> 2, py = (par >> 1) & 1, pz = par & 1;
+      const int nz = par_taps(pz), ny = par_taps(py);
+      const int jz = kk % nz, jy = (kk / nz) % ny, jx = kk / (nz * ny);
+      const int tx = px - 2 * par_e(px, jx) + 2, ty = py - 2 * par_e(py, jy) + 2, tz = pz - 2 * par_e(pz, jz) + 2;
+      w = a.G[c * 216 + (tx * 6 + ty) * 6 + tz];
+    }
+    sW[e] = w;
+  }
+  __syncthreads();
+  const int m0 = a.n0 >> 1, m1 = a.n1 >> 1, m2 = a.n2 >> 1;
+  const int m12 = m1 * m2, m012 = m12 * m0;
+  const int I = blockIdx.x;
+  const int64_t b = blockIdx.y;
+  const float* cb = a.xc + b * 16 * (int64_t)m012;
+  float* yb = a.y + b * 8 * (int64_t)m012;
+  const int n2 = a.n2, n12 = a.n1 * a.n2;
+  int po[3];
+#pragma unroll
+  for (int e = 0; e < 3; ++e) po[e] = pw(I - 1 + e, m0) * m12;
+  for (int q = tid; q < m12; q += blockDim.x) {
+    const int J1 = q / m2, J2 = q - J1 * m2;
+    int ro[3], co[3];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      ro[e] = pw(J1 - 1 + e, m1) * m2;
+      co[e] = pw(J2 - 1 + e, m2);
+    }
+    float acc[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) acc[p] = 0.f;
+#pragma unroll 1
+    for (int c = 0; c < 16; ++c) {
+      const float* xc = cb + c * m012;
+      float v[3][3][3];
+#pragma unroll
+      for (int e0 = 0; e0 < 3; ++e0)
+#pragma unroll
+        for (int e1 = 0; e1 < 3; ++e1)
+#pragma unroll
+          for (int e2 = 0; e2 < 3; ++e2) v[e0][e1][e2] = __ldg(xc + po[e0] + ro[e1] + co[e2]);
+      const float4* w4 = reinterpret_cast<const float4*>(sW + c * 128);
+      int k = 0;
+#pragma unroll
+      for (int par = 0; par < 8; ++par) {
+        const int px = par >> 2, py = (par >> 1) & 1, pz = par & 1;
+#pragma unroll
+        for (int jx = 0; jx < par_taps(px); ++jx)
+#pragma unroll
+          for (int jy = 0; jy < par_taps(py); ++jy)
+#pragma unroll
+            for (int jz = 0; jz < par_taps(pz); ++jz, ++k) {
+              const float4 w = w4[k >> 2];
+              const float wk = (k & 3) == 0 ? w.x : ((k & 3) == 1 ? w.y : ((k & 3) == 2 ? w.z : w.w));
+              acc[par] = fmaf(wk, v[par_e(px, jx) + 1][par_e(py, jy) + 1][par_e(pz, jz) + 1], acc[par]);
+            }
+      }
+    }
+    float* yp = yb + (int64_t)(2 * I) * n12 + (2 * J1) * n2 + 2 * J2;
+#pragma unroll
+    for (int par = 0; par < 8; ++par) {
+      float* o = yp + (par >> 2) * n12 + ((par >> 1) & 1) * n2 + (par & 1);
+      *o += acc[par];
+    }
+  }
+}
+
 template <typename KernelT>
 int launch_fine(KernelT k, const FoldArgs& a, const char* what, cudaStream_t st) {
   const int nkx = (a.n2 + 31) / 32;
@@ -439,7 +543,15 @@ int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* x
     }
     return launch_fine(fold_fine_kernel<1, 1>, a, "fold_fine_kernel<1,1>", st);
   }
-  if (rh == 2 && cc == 16) return launch_fine(fold_fine_kernel<2, 16>, a, "fold_fine_kernel<2,16>", st);
+  if (rh == 2 && cc == 16) {
+    // fine 5^3 part, then the coarse part added as a parity convolution
+    int rc = launch_fine(fold_fine_kernel<2, 0>, a, "fold_fine_kernel<2,0>", st);
+    if (rc) return rc;
+    const int m12 = (int)(n_c[1] / 2 * (n_c[2] / 2));
+    const unsigned threads = (unsigned)std::min(256, (m12 + 31) / 32 * 32);
+    fold_parity16_kernel<<<dim3((unsigned)(n_c[0] / 2), (unsigned)nb), threads, 0, st>>>(a);
+    return check_launch("fold_parity16_kernel");
+  }
   return fail(GB_E_UNSUPPORTED, "gb_learned_fold_fine: (rh, cc) not in {(1, 1), (2, 16)}");
 }
 
