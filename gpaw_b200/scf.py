@@ -25,6 +25,7 @@ for comparing precision modes of one geometry).
 """
 from __future__ import annotations
 
+import gc
 import time
 from dataclasses import dataclass, field
 
@@ -497,13 +498,22 @@ class _GraphedIteration:
         side.wait_stream(torch.cuda.current_stream())
         self.gA = torch.cuda.CUDAGraph()
         self.gB = torch.cuda.CUDAGraph()
-        with torch.cuda.stream(side):
-            self.gA.capture_begin(pool=self.pool)
-            self.H, self.Htpsit = es.subspace_matrix(calc, wfs, kpt)
-            self.gA.capture_end()
-            self.gB.capture_begin(pool=self.pool)
-            self._capture_b(calc, wfs, kpt, es, weights)
-            self.gB.capture_end()
+        # no cyclic garbage collection while capturing: a collection would
+        # pause the host for as long as the heap is big and could free
+        # device tensors in the middle of the capture
+        gc_on = gc.isenabled()
+        gc.disable()
+        try:
+            with torch.cuda.stream(side):
+                self.gA.capture_begin(pool=self.pool)
+                self.H, self.Htpsit = es.subspace_matrix(calc, wfs, kpt)
+                self.gA.capture_end()
+                self.gB.capture_begin(pool=self.pool)
+                self._capture_b(calc, wfs, kpt, es, weights)
+                self.gB.capture_end()
+        finally:
+            if gc_on:
+                gc.enable()
         torch.cuda.current_stream().wait_stream(side)
         kpt.psit_nG = self.psit
         kpt.P_nM = self.P
