@@ -406,33 +406,41 @@ __global__ void __launch_bounds__(256) fold_stride_kernel(const StrideArgs a) {
 // every CTA stages G reordered into the order the unrolled loops consume it
 // (channel, parity, tap), 128 floats per channel, so each 16-byte broadcast
 // shared load serves four FMAs.
-constexpr int NPAR = 125;   // (3 + 2)^3 taps over the 8 parities
-
-__device__ __forceinline__ constexpr int par_taps(int p) { return p ? 2 : 3; }
+__host__ __device__ __forceinline__ constexpr int par_taps(int p) { return p ? 2 : 3; }
 // e of the j-th tap of parity p: p = 0 -> -1, 0, 1; p = 1 -> 0, 1
-__device__ __forceinline__ constexpr int par_e(int p, int j) { return p ? j : j - 1; }
+__host__ __device__ __forceinline__ constexpr int par_e(int p, int j) { return p ? j : j - 1; }
+
+// index into G[c][6][6][6] of the k-th weight in (parity, tap) order, the
+// order of the unrolled loops below: (3 + 2)^3 = 125 over the 8 parities,
+// then -1
+struct ParityTaps {
+  int v[128];
+};
+constexpr ParityTaps make_parity_taps() {
+  ParityTaps t{};
+  int k = 0;
+  for (int par = 0; par < 8; ++par) {
+    const int px = par >> 2, py = (par >> 1) & 1, pz = par & 1;
+    for (int jx = 0; jx < par_taps(px); ++jx)
+      for (int jy = 0; jy < par_taps(py); ++jy)
+        for (int jz = 0; jz < par_taps(pz); ++jz) {
+          const int tx = px - 2 * par_e(px, jx) + 2, ty = py - 2 * par_e(py, jy) + 2;
+          const int tz = pz - 2 * par_e(pz, jz) + 2;
+          t.v[k++] = (tx * 6 + ty) * 6 + tz;
+        }
+  }
+  for (; k < 128; ++k) t.v[k] = -1;
+  return t;
+}
+__constant__ ParityTaps kParityTaps = make_parity_taps();
 
 __global__ void __launch_bounds__(256) fold_parity16_kernel(const FoldArgs a) {
   __shared__ __align__(16) float sW[16 * 128];
   const int tid = threadIdx.x;
   // reorder G[c][tx][ty][tz] (t in 0..5) into (c, parity, tap) order
   for (int e = tid; e < 16 * 128; e += blockDim.x) {
-    const int c = e >> 7, k = e & 127;
-    float w = 0.f;
-    if (k < NPAR) {
-      int kk = k, par = 0;
-      for (; par < 8; ++par) {
-        const int n = par_taps(par >> 2) * par_taps((par >> 1) & 1) * par_taps(par & 1);
-        if (kk < n) break;
-        kk -= n;
-      }
-      const int px = par >> 2, py = (par >> 1) & 1, pz = par & 1;
-      const int nz = par_taps(pz), ny = par_taps(py);
-      const int jz = kk % nz, jy = (kk / nz) % ny, jx = kk / (nz * ny);
-      const int tx = px - 2 * par_e(px, jx) + 2, ty = py - 2 * par_e(py, jy) + 2, tz = pz - 2 * par_e(pz, jz) + 2;
-      w = a.G[c * 216 + (tx * 6 + ty) * 6 + tz];
-    }
-    sW[e] = w;
+    const int src = kParityTaps.v[e & 127];
+    sW[e] = src >= 0 ? __ldg(a.G + (e >> 7) * 216 + src) : 0.f;
   }
   __syncthreads();
   const int m0 = a.n0 >> 1, m1 = a.n1 >> 1, m2 = a.n2 >> 1;
