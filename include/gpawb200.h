@@ -238,7 +238,9 @@ int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw,
  *   fine:   y[p] = sum_{|d|<=rh} F[d] xf[p + d]
  *                + sum_{c<cc} sum_{e in {-1,0,1}^3} G[c][(p%2) - 2e + 2] xc[c][p/2 + e]
  *           F: (2rh+1)^3, G: cc x 6^3 ([c][tx][ty][tz]); (rh, cc) in
- *           {(1, 1), (2, 16)}; xc (nb, cc, n/2) per axis; n2 >= 10
+ *           {(1, 1), (2, 16)}; xc (nb, cc, n/2) per axis; n2 >= 10;
+ *           y must not overlap xf or xc (for (2, 16) the fine part is
+ *           written first and the coarse part added by a second launch)
  *   stride: y[c][I] = sum_{|d|<=2} Q[d][c] x[2I + d], 16 channels out,
  *           Q [125][16], y (nb, 16, n/2) per axis */
 int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* xc,
