@@ -15,7 +15,7 @@ Also reported on the same JSON line:
   e2e          the same metric through the public API with host buffers
                (pinned H2D copy + apply + D2H copy inside the timed region)
   cpu_baseline GPAW's own C Operator (built from the reference sources into
-               oracle/_ref) on the host cores, bounded sample of 16 grids
+               oracle/_ref) on the host cores, the full 256-grid step
 
 `--impl reference` times GPAW's own C implementation of the same step on the
 host cores (all threads) and prints the same metric with "impl": "reference".
@@ -28,7 +28,6 @@ import argparse
 import gc
 import json
 import os
-import re
 import subprocess
 import sys
 import threading
@@ -54,16 +53,18 @@ def peaks():
     return 6650.0, 'fallback'
 
 
+# DRAM bytes per 96^3 FP64 grid of one stencil launch
+# (dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of a 64-grid
+# launch of the same kernel, divided by 64; the capture is summarised in
+# profiles/star_tma_kernel_f64_laplace_96cubed.txt)
+STENCIL_TRAFFIC_PER_GRID = 16.35e6
+
+
 def profiled_traffic(nb):
-    """DRAM bytes per launch of the stencil kernel: the per-grid figure of
-    the committed ncu summary (profiles/star_tma_kernel_f64_laplace_96cubed.txt,
-    a capture of a smaller batch of the same 96^3 grids; traffic grows in
-    proportion to the grids per launch) times the grids per launch, or None."""
-    p = REPO / 'profiles' / 'star_tma_kernel_f64_laplace_96cubed.txt'
-    if not p.exists():
-        return None
-    m = re.search(r'traffic_bytes_per_grid\s*=\s*([0-9.eE+]+)', p.read_text())
-    return round(float(m.group(1)) * nb) if m else None
+    """DRAM bytes per launch of the stencil kernel: the per-grid traffic of
+    the ncu capture times the grids per launch (traffic grows in proportion
+    to the grids per launch)."""
+    return round(STENCIL_TRAFFIC_PER_GRID * nb)
 
 
 class ClockSampler:
@@ -496,63 +497,55 @@ def band_gemm_benchmark(args):
     print(json.dumps(out))
 
 
-def cpu_reference_rate(nb_sample, threads, reps=3):
-    """GPAW's own C Operator (oracle/_ref) on the host: best-of GB/s."""
+def cpu_reference_run(nb, steps, warmup):
+    """GPAW's own C Operator (oracle/_ref, OpenMP over the host cores) on the
+    benchmark step: the order-6 Laplacian of `nb` periodic 96^3 FP64 grids,
+    seeded N(0, 1).  `warmup` untimed applications, then the mean over
+    `steps` timed ones (time.perf_counter).  Both the reference arm and the
+    cpu_baseline of this arm use this one method.  Returns (GB/s, seconds
+    per step) or None where the reference build is absent."""
     from oracle import ref, fd
     if not ref.available():
         return None
     gd = grid(True)
     coefs, offs = fd.guc_laplace(gd.h_cv, -0.5, 3)
     op = ref.operator(coefs, offs, gd.n_c, (1, 1, 1), True)
-    rng = np.random.default_rng(0)
-    a = rng.standard_normal((nb_sample,) + tuple(gd.n_c))
+    a = np.random.default_rng(0).standard_normal((nb,) + tuple(gd.n_c))
     b = np.zeros_like(a)
-    op.apply(a, b)
-    best = 1e30
-    for _ in range(reps):
-        t0 = time.perf_counter()
+    for _ in range(max(warmup, 1)):
         op.apply(a, b)
-        best = min(best, time.perf_counter() - t0)
-    return 2 * a.nbytes / best / 1e9, best
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        op.apply(a, b)
+    t = (time.perf_counter() - t0) / steps
+    return 2 * a.nbytes / t / 1e9, t
 
 
 def run_reference(args):
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    from oracle import ref
-    if not ref.available():
+    threads = int(os.environ.get('OMP_NUM_THREADS', os.cpu_count() or 1))
+    r = cpu_reference_run(NB, args.steps, args.warmup)
+    if r is None:
         print(json.dumps({'impl': 'reference', 'unavailable':
                           'oracle/_ref (GPAW C extension from the reference '
                           'sources) was not built'}))
         return
-    nb = 16
-    from oracle import fd
-    gd = grid(True)
-    coefs, offs = fd.guc_laplace(gd.h_cv, -0.5, 3)
-    op = ref.operator(coefs, offs, gd.n_c, (1, 1, 1), True)
-    rng = np.random.default_rng(0)
-    a = rng.standard_normal((nb,) + tuple(gd.n_c))
-    b = np.zeros_like(a)
-    for _ in range(args.warmup):
-        op.apply(a, b)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        op.apply(a, b)
-    t = time.perf_counter() - t0
-    value = 2 * a.nbytes * args.steps / t / 1e9
+    value, t = r
     line = {
         'impl': 'reference', 'metric': METRIC, 'value': round(value, 2),
         'unit': 'GB/s', 'n_gpus': args.gpus, 'steps': args.steps,
-        'warmup': args.warmup, 'ms_per_step': round(t / args.steps * 1e3, 3),
+        'warmup': args.warmup, 'ms_per_step': round(t * 1e3, 3),
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f64', 'data': 'synthetic N(0,1), seed 0',
-        'config': {'workload': 'laplace_nn3_f64_periodic_256x96^3',
-                   'sample': f'{nb} of 256 grids per step'},
+        'config': {'workload': f'laplace_nn3_f64_periodic_{NB}x96^3',
+                   'sample': f'the full {NB}-grid step, mean of {args.steps} '
+                             f'after {max(args.warmup, 1)} warm-up'},
         'cpu_baseline': {'value': round(value, 2), 'unit': 'GB/s',
                          'cores': threads, 'kind': 'reference',
-                         'sample': f'{nb} grids of 96^3 per step'},
+                         'sample': f'{NB} grids of 96^3 per step, mean of '
+                                   f'{args.steps} steps'},
         'e2e': {'value': round(value, 2), 'unit': 'GB/s',
                 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
@@ -595,8 +588,10 @@ def main():
     args = ap.parse_args()
     if args.dtype != 'f64' and not args.kernel_only:
         ap.error('--dtype f32 is for --kernel-only runs; the benchmark line is FP64')
+    # GPAW's C operator (the reference arm and the cpu_baseline) runs OpenMP
+    # over every host core; set before the extension is loaded
+    os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count() or 1))
     if args.impl == 'reference':
-        os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count() or 1))
         run_reference(args)
         return
     if args.network_only:
@@ -724,14 +719,14 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1:
-        threads = os.cpu_count() or 1
-        r = cpu_reference_rate(16, threads)
+        threads = int(os.environ.get('OMP_NUM_THREADS', os.cpu_count() or 1))
+        r = cpu_reference_run(NB, 3, 1)
         if r is not None:
             cpu = {'value': round(r[0], 2), 'unit': 'GB/s', 'cores': threads,
                    'kind': 'reference',
-                   'sample': '16 grids of 96^3 FP64 periodic, best of 3 '
-                             '(GPAW C Operator from the reference sources, '
-                             f'OpenMP {os.environ.get("OMP_NUM_THREADS", "default")} threads)'}
+                   'sample': f'the full {NB}-grid step of 96^3 FP64 periodic grids, '
+                             'mean of 3 after 1 warm-up (GPAW C Operator from the '
+                             f'reference sources, OpenMP {threads} threads)'}
 
     peak, peak_kind = peaks()
     achieved = nbytes / (launch_ms / 1e3) / 1e9

@@ -534,6 +534,19 @@ int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* x
   GB_REQUIRE(xc && G, "gb_learned_fold_fine: missing coarse input or weights");
   GB_REQUIRE(nb < 65536 && n_c[0] * n_c[1] * n_c[2] * (cc > 1 ? cc : 1) < ((int64_t)1 << 31),
              "gb_learned_fold_fine: too many grids or points per grid");
+  {
+    // y is written (fine part) before the coarse part reads xc and adds
+    // into y, so an output overlapping either input gives wrong results
+    const uint64_t nf = (uint64_t)nb * n_c[0] * n_c[1] * n_c[2] * sizeof(float);
+    const uint64_t nco = (uint64_t)nb * (cc > 1 ? cc : 1) * (n_c[0] / 2) * (n_c[1] / 2) * (n_c[2] / 2) *
+                         sizeof(float);
+    auto overlap = [](const void* a, uint64_t na, const void* b, uint64_t nb_) {
+      const uint64_t pa = (uint64_t)(uintptr_t)a, pb = (uint64_t)(uintptr_t)b;
+      return pa < pb + nb_ && pb < pa + na;
+    };
+    GB_REQUIRE(!overlap(y, nf, xf, nf) && !overlap(y, nf, xc, nco),
+               "gb_learned_fold_fine: the output overlaps an input");
+  }
   FoldArgs a{xf, xc, y, F, G, nb, (int)n_c[0], (int)n_c[1], (int)n_c[2]};
   cudaStream_t st = (cudaStream_t)stream;
   if (rh == 1 && cc == 1) {

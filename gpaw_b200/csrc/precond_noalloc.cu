@@ -13,7 +13,14 @@
 // until the process exits.  Host code cannot use its name as a device
 // address; the first call on each device looks the address up with
 // cudaGetSymbolAddress while that device is current and keeps it.  Make that
-// first call before any stream capture begins on the device.
+// first call before any stream capture begins on the device.  With CUDA's
+// lazy module loading (CUDA_MODULE_LOADING=LAZY, the default since 12.2) the
+// array is only placed in device memory by that first look-up, so a caller
+// whose budget is fixed at start-up makes one call at start-up: a call with
+// nin = 0 does the look-up and launches nothing.  The kept address belongs
+// to the device's primary context: after cudaDeviceReset (or a reset of the
+// primary context) it is stale, and this entry point must not be called on
+// that device again in the same process.
 //
 // Size: q0 (one level-0 grid per band), r1, d1, q1 (level 1) and r2, d2
 // (level 2), each rounded up to 256 bytes -- about 1.41 x nin x level-0
@@ -72,9 +79,17 @@ extern "C" int gb_fd_precond_noalloc(const gb_transformer* rest0, const gb_trans
                                      const double* phase_cd, void* stream) {
   GB_REQUIRE(kin0 && kin1 && kin2, "gb_fd_precond_noalloc: null operator");
   GB_REQUIRE(dtype_valid(dtype) && nin >= 0, "gb_fd_precond_noalloc: bad dtype or batch");
-  if (nin == 0) return GB_OK;
+  void* base = nullptr;
+  if (nin == 0) return scratch_address(&base);  // set-up only
   GB_REQUIRE(d0 && residuals, "gb_fd_precond_noalloc: null residuals or output");
   const size_t es = dtype_size(dtype);
+  const size_t points0 = (size_t)(kin0->n[0] * kin0->n[1] * kin0->n[2]);
+  // a batch whose level-0 grids alone exceed the array is refused before any
+  // product that could wrap around
+  if (points0 == 0 || (size_t)nin > PRECOND_SCRATCH_BYTES / (points0 * es))
+    return fail(GB_E_INVALID, "gb_fd_precond_noalloc: " + std::to_string(nin) +
+                                  " grids need more work space than the fixed " +
+                                  std::to_string(PRECOND_SCRATCH_BYTES) + " bytes; pass fewer grids per call");
   auto level_bytes = [&](const gb_operator* k) {
     return round256((size_t)nin * (size_t)(k->n[0] * k->n[1] * k->n[2]) * es);
   };
@@ -84,7 +99,6 @@ extern "C" int gb_fd_precond_noalloc(const gb_transformer* rest0, const gb_trans
     return fail(GB_E_INVALID, "gb_fd_precond_noalloc: " + std::to_string(nin) + " grids need " +
                                   std::to_string(need) + " bytes of work space, more than the fixed " +
                                   std::to_string(PRECOND_SCRATCH_BYTES) + " bytes; pass fewer grids per call");
-  void* base = nullptr;
   int rc = scratch_address(&base);
   if (rc) return rc;
   unsigned char* p = static_cast<unsigned char*>(base);

@@ -9,14 +9,17 @@ Same classes and signatures as the reference (gpaw/fd_operators.py:36-309):
 complex128/complex64 for ``dtype=complex``.  The stencil itself runs in
 libgpawb200 (gb_operator_*), one launch for all leading (band, k) dims.
 
-The stencil coefficients are rebuilt here from the mathematics the reference
-uses: Chelikowsky et al., Phys. Rev. B 50, 11355 (1994) central-difference
-weights for the Laplacian and first derivative, a least-squares fit of the
-second-derivative identity over the shortest lattice directions for general
-cells, and Voronoi nearest neighbours for gradients.
+The stencil coefficients are derived here from the mathematics:
+central-difference weights of order 2n for the second and first derivative
+(exact Taylor matching, as tabulated by Chelikowsky et al., Phys. Rev. B 50,
+11355 (1994)); for general cells the Laplacian is a combination of
+second derivatives along the shortest grid steps whose second-moment
+tensors sum to the identity, and the gradient combines first differences
+along the steps to the Voronoi neighbours of a grid point.
 """
 from __future__ import annotations
 
+import itertools
 from fractions import Fraction
 
 import numpy as np
@@ -177,6 +180,120 @@ class FDOperator:
         return (0, 1, 1)
 
 
+def _half_space_steps():
+    """The 13 grid steps M in {-1, 0, 1}^3 that are lexicographically
+    positive (one of each +-M pair), in lexicographic order."""
+    return np.array([m for m in itertools.product((-1, 0, 1), repeat=3)
+                     if m > (0, 0, 0)])
+
+
+def _second_moments(E_dv):
+    """Rows xx, yy, zz, yz, xz, xy of the tensors e_d e_d^T (one column per
+    step vector e_d)."""
+    x, y, z = E_dv.T
+    return np.array([x * x, y * y, z * z, y * z, x * z, x * y])
+
+
+def laplace_stencil(h_cv, scale=1.0, n=1):
+    """(coef_p, offset_pc) of the order-2n Laplacian on a general grid.
+
+    nabla^2 = sum_d a_d (e_d . nabla)^2 holds exactly when the step vectors
+    e_d (lattice steps M_d h_cv) satisfy sum_d a_d e_d e_d^T = 1, six
+    equations in the a_d.  The steps are taken shortest first, where
+    "short" is measured on the grid axes normalised to unit length (so
+    the choice depends on the angles between the axes, not on their
+    spacing), with ties kept in lexicographic order; the first 3, 4, 5 or 6
+    of them whose moment equations have an exact solution are used, and a
+    set whose moment tensors are linearly dependent is an error, as in the
+    reference (gpaw/fd_operators.py:179-235).  Along each step the 1-D
+    order-2n second-derivative weights apply: centre sum_d a_d w_0, then
+    a_d w_k at +-k M_d."""
+    h_cv = np.asarray(h_cv, float)
+    steps = _half_space_steps()
+    axes = h_cv / np.linalg.norm(h_cv, axis=1)[:, None]
+    length2 = ((steps @ axes)**2).sum(1)
+    order = np.argsort(length2, kind='stable')
+    target = np.array([1.0, 1.0, 1.0, 0.0, 0.0, 0.0])
+    for D in range(3, 7):
+        M_d = steps[order[:D]]
+        A = _second_moments(M_d @ h_cv)              # (6, D)
+        Q, R = np.linalg.qr(A)
+        sv = np.linalg.svd(A, compute_uv=False)
+        if sv[-1] <= sv[0] * 1e-12:
+            raise ValueError('You have a weird unit cell!  Try to use the '
+                             'maximally reduced Niggli cell.')
+        a_d = np.linalg.solve(R, Q.T @ target)
+        if D == 6 or ((A @ a_d - target)**2).sum() < 1e-14:
+            break
+    a_d = a_d * scale
+    w = laplace[n]
+    coefs = [w[0] * a_d.sum()]
+    offsets = [np.zeros(3, int)]
+    for a, M in zip(a_d, M_d):
+        for sign in (1, -1):
+            for k in range(1, n + 1):
+                offsets.append(sign * k * M)
+                coefs.append(a * w[k])
+    return np.array(coefs), np.array(offsets).reshape(-1, 3)
+
+
+def _voronoi_relevant_steps(h_cv):
+    """Steps M (one of each +-M pair, lexicographic order) whose grid point
+    shares a face of positive area with the Voronoi cell of the origin,
+    among the 27 points {-1, 0, 1}^3 h_cv.  The face between 0 and p is
+    symmetric about p / 2, so it has positive area exactly when p / 2 is
+    strictly closer to 0 and p than to every other point q:
+    q . (q - p) > 0 (up to rounding)."""
+    pts = np.array(list(itertools.product((-1, 0, 1), repeat=3))) @ h_cv
+    tol = 1e-10 * (np.asarray(h_cv)**2).sum(1).max()
+    out = []
+    for M in _half_space_steps():
+        p = M @ h_cv
+        others = [q for q in pts if np.any(np.abs(q) > 0) and
+                  np.any(np.abs(q - p) > 1e-14 * np.abs(p).max())]
+        if all(q @ (q - p) > tol for q in others):
+            out.append(M)
+    return np.array(out)
+
+
+def gradient_stencil(h_cv, v, scale=1.0, n=1):
+    """(coef_p, offset_pc) of the order-2n derivative along Cartesian axis
+    v on a general grid.
+
+    Uses the steps M_d to the Voronoi neighbours of a grid point.  For each
+    grid axis c, n_c is the unit normal of the plane of the two other axes
+    (the normalised reciprocal vector); the weights b_cd are the
+    minimum-norm solution of sum_d b_cd e_d = n_c over the steps not lying
+    in that plane (e_d = M_d h_cv), so that sum_d b_cd (f(r + e_d) -
+    f(r - e_d)) / 2 approximates n_c . grad f.  The Cartesian derivative is
+    the combination sum_c (N^-1)_vc of these (N the matrix of the n_c), and
+    each step carries the 1-D order-2n first-derivative weights
+    (gpaw/fd_operators.py:238-303 builds the same operator)."""
+    h_cv = np.asarray(h_cv, float)
+    M_d = _voronoi_relevant_steps(h_cv)
+    E_dv = M_d @ h_cv
+    recip = np.linalg.inv(h_cv).T                     # rows: reciprocal vectors
+    N_cv = recip / np.linalg.norm(recip, axis=1)[:, None]
+    b_cd = np.zeros((3, len(M_d)))
+    for c in range(3):
+        use = np.abs(E_dv @ N_cv[c]) > 1e-10
+        B = E_dv[use].T                               # (3, m) steps as columns
+        # n_c lies in the span of the steps used; lstsq gives the
+        # minimum-norm weights also when they span less than 3 dimensions
+        b_cd[c, use] = np.linalg.lstsq(B, N_cv[c], rcond=None)[0]
+    coef_d = np.linalg.inv(N_cv)[v] @ b_cd * scale
+    d_k = derivatives[n - 1]
+    coefs, offsets = [], []
+    for c, M in zip(coef_d, M_d):
+        if abs(c) < 1e-10:
+            continue
+        for sign in (1, -1):
+            for k in range(1, n + 1):
+                offsets.append(sign * k * M)
+                coefs.append(sign * c * d_k[k - 1])
+    return np.array(coefs), np.array(offsets).reshape(-1, 3)
+
+
 def Laplace(gd, scale=1.0, n=1, dtype=float, xp=None):
     if n == 9:
         raise NotImplementedError('FTLaplace (n=9) is not part of this build')
@@ -185,84 +302,20 @@ def Laplace(gd, scale=1.0, n=1, dtype=float, xp=None):
 
 class GUCLaplace(FDOperator):
     def __init__(self, gd, scale=1.0, n=1, dtype=float, xp=None):
-        """Laplacian for a general (possibly non-orthorhombic) cell.
-
-        The second-derivative identity sum_d a_d (h_d . grad)^2 = nabla^2 is
-        fitted by least squares over the D = 3..6 shortest lattice directions
-        (the same construction as gpaw/fd_operators.py:192-216); each
-        direction then gets the 1-D order-2n weights."""
-        M_ic = np.indices((3, 3, 3)).reshape((3, -3)).T[-13:] - 1
-        u_cv = gd.h_cv / (gd.h_cv**2).sum(1)[:, np.newaxis]**0.5
-        u2_i = (np.dot(M_ic, u_cv)**2).sum(1)
-        i_d = u2_i.argsort()
-        m_mv = np.array([(2, 0, 0), (0, 2, 0), (0, 0, 2),
-                         (0, 1, 1), (1, 0, 1), (1, 1, 0)])
-        for D in range(3, 7):
-            h_dv = np.dot(M_ic[i_d[:D]], gd.h_cv)
-            A_md = (h_dv**m_mv[:, np.newaxis, :]).prod(2)
-            a_d, residual, rank, s = np.linalg.lstsq(
-                A_md, [1, 1, 1, 0, 0, 0], rcond=-1)
-            if residual.sum() < 1e-14:
-                if rank != D:
-                    raise ValueError('You have a weird unit cell!  Try to use '
-                                     'the maximally reduced Niggli cell.')
-                break
-        a_d *= scale
-        offsets = [(0, 0, 0)]
-        coefs = [laplace[n][0] * a_d.sum()]
-        for d in range(D):
-            M_c = M_ic[i_d[d]]
-            offsets.extend(np.arange(1, n + 1)[:, np.newaxis] * M_c)
-            coefs.extend(a_d[d] * np.array(laplace[n][1:]))
-            offsets.extend(np.arange(-1, -n - 1, -1)[:, np.newaxis] * M_c)
-            coefs.extend(a_d[d] * np.array(laplace[n][1:]))
+        """Order-2n Laplacian for a general (possibly non-orthorhombic)
+        grid; coefficients from `laplace_stencil`."""
+        coefs, offsets = laplace_stencil(gd.h_cv, scale, n)
         FDOperator.__init__(self, coefs, offsets, gd, dtype, xp=xp)
-        self.description = (
-            '%d*%d+1=%d point O(h^%d) finite-difference Laplacian' %
-            ((self.npoints - 1) // n, n, self.npoints, 2 * n))
+        ndir = (self.npoints - 1) // (2 * n)
+        self.description = (f'{ndir} directions x {2 * n} + 1 = {self.npoints} '
+                            f'point O(h^{2 * n}) finite-difference Laplacian')
 
 
 class Gradient(FDOperator):
     def __init__(self, gd, v, scale=1.0, n=1, dtype=float, xp=None):
-        """Symmetric gradient along Cartesian direction v for a general cell
-        (Voronoi nearest neighbours + a 3x3 solve per lattice direction, as
-        gpaw/fd_operators.py:251-303)."""
-        from scipy.spatial import Voronoi
-        M_ic = np.indices((3, 3, 3)).reshape((3, -1)).T - 1
-        h_iv = M_ic.dot(gd.h_cv)
-        voro = Voronoi(h_iv)
-        i_d = []
-        for i1, i2 in voro.ridge_points:
-            if i1 == 13 and i2 > 13:
-                i_d.append(i2)
-            elif i2 == 13 and i1 > 13:
-                i_d.append(i1)
-        D = len(i_d)
-        h_dv = h_iv[i_d]
-        invh_vc = np.linalg.inv(gd.h_cv)
-        n_cv = (invh_vc / (invh_vc**2).sum(axis=0)**0.5).T
-        coef_cd = np.zeros((3, D))
-        for c, n_v in enumerate(n_cv):
-            ok_d = abs(h_dv.dot(n_v)) > 1e-10
-            h_mv = h_dv[ok_d]
-            A_jm = np.array([h_mv.dot(n_v), h_mv.dot(gd.h_cv[c - 1]),
-                             h_mv.dot(gd.h_cv[c - 2])])
-            U_jm, S_m, V_mm = np.linalg.svd(A_jm, full_matrices=False)
-            coef_cd[c, ok_d] = V_mm.T.dot(np.diag(S_m**-1).dot(
-                U_jm.T.dot([1, 0, 0])))
-        coef_d = np.linalg.inv(n_cv)[v].dot(coef_cd) * scale
-        offsets = []
-        coefs = []
-        stencil = np.array(derivatives[n - 1])
-        for d, c in enumerate(coef_d):
-            if abs(c) < 1e-10:
-                continue
-            M_c = M_ic[i_d[d]]
-            offsets.extend(np.arange(1, n + 1)[:, np.newaxis] * M_c)
-            coefs.extend(c * stencil)
-            offsets.extend(np.arange(-1, -n - 1, -1)[:, np.newaxis] * M_c)
-            coefs.extend(-c * stencil)
+        """Order-2n derivative along Cartesian axis v for a general grid;
+        coefficients from `gradient_stencil`."""
+        coefs, offsets = gradient_stencil(gd.h_cv, v, scale, n)
         FDOperator.__init__(self, coefs, offsets, gd, dtype, xp=xp)
-        self.description = (
-            'Finite-difference {}-derivative with O(h^{}) error ({} points)'
-            .format('xyz'[v], 2 * n, self.npoints))
+        self.description = (f'O(h^{2 * n}) finite-difference derivative along '
+                            f'{"xyz"[v]} ({self.npoints} points)')

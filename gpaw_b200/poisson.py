@@ -78,9 +78,9 @@ class FastPoissonSolver:
                 a = re + 1j * im if a.is_complex() else re
         return a
 
-    def solve(self, phi_g, rho_g, charge=None, eps=None, maxcharge=1e-6,
-              zero_initial_phi=False, timer=None):
-        """phi_g <- solution of (-1/(4 pi)) L phi = rho (the neutral part)."""
+    def solve_neutral(self, phi_g, rho_g, timer=None):
+        """phi_g <- the solution of (-1/(4 pi)) L phi = rho_g, rho_g taken
+        as given (gpaw/poisson.py:957-1002)."""
         if self.gd is None:
             raise RuntimeError('set_grid_descriptor first')
         assert rho_g.dtype == torch.float64, 'the Poisson solve stays FP64'
@@ -91,4 +91,45 @@ class FastPoissonSolver:
         phi_g.copy_(a.real if a.is_complex() else a)
         return 1
 
-    solve_neutral = solve
+    def _gaussian(self):
+        """The normalised L = 0 Gaussian at the cell centre and its
+        potential (gpaw/utilities/gauss.py:95-139 with a = 19; r^2 clamped
+        at 1e-12, gpaw/utilities/tools.py:96-115)."""
+        if getattr(self, '_gauss', None) is None:
+            gd = self.gd
+            icell_cv = np.linalg.inv(gd.cell_cv).T
+            a = 4 * 19.0 * (icell_cv**2).sum(1).max()
+            idx = np.indices(tuple(gd.n_c)).reshape(3, -1).T + gd.beg_c
+            r_v = idx @ gd.h_cv - 0.5 * gd.cell_cv.sum(0)
+            r2 = np.maximum((r_v**2).sum(1), 1e-12)
+            r = torch.from_numpy(np.sqrt(r2))
+            g = np.sqrt(4 * a**3) / np.pi * np.exp(-a * r2)
+            phi = 2 * np.sqrt(np.pi) * torch.special.erf(np.sqrt(a) * r) / r
+            self._gauss = (torch.from_numpy(g).reshape(tuple(gd.n_c)).to(gd.device),
+                           phi.reshape(tuple(gd.n_c)).to(gd.device))
+        return self._gauss
+
+    def solve(self, phi_g, rho_g, charge=None, eps=None, maxcharge=1e-6,
+              zero_initial_phi=False, timer=None):
+        """phi_g <- the potential of rho_g (gpaw/poisson.py:178-279): a
+        uniform background equal to the mean of rho_g is subtracted from
+        neutral systems (|charge| <= maxcharge) and from periodic ones; a
+        charged zero-boundary system is neutralised with a Gaussian whose
+        analytic potential is added back; charged systems with mixed
+        boundaries are not supported.  charge=None reads the charge from
+        rho_g (one device-to-host read); a caller that knows its density
+        is neutral passes charge=0 and the solve stays on the device."""
+        if self.gd is None:
+            raise RuntimeError('set_grid_descriptor first')
+        background = rho_g.mean()
+        if charge is None:
+            charge = float(rho_g.sum()) * self.gd.dv
+        if abs(charge) <= maxcharge or all(self.gd.pbc_c):
+            return self.solve_neutral(phi_g, rho_g - background)
+        if any(self.gd.pbc_c):
+            raise NotImplementedError('charged system with mixed boundary conditions')
+        g, phi_gauss = self._gaussian()
+        q = float(rho_g.sum()) * self.gd.dv / np.sqrt(4 * np.pi)
+        self.solve_neutral(phi_g, rho_g - q * g)
+        phi_g.add_(q * phi_gauss)
+        return 1

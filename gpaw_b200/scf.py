@@ -269,9 +269,9 @@ class Calculation:
         Ntot = nt_g.sum() * finegd.dv
         nt_g *= self.nvalence / Ntot.clamp_min(1e-300)
         rhot_g = nt_g + self.rhoion_g
-        if self.pbc.all():
-            rhot_g = rhot_g - rhot_g.mean()
-        self.poisson.solve(self.vHt_g, rhot_g)
+        # a neutral system: the solver subtracts the mean (the uniform
+        # background) and stays on the device
+        self.poisson.solve(self.vHt_g, rhot_g, charge=0.0)
         vxc_g = torch.zeros((1,) + tuple(finegd.n_c), dtype=torch.float64,
                             device=finegd.device)
         e_g = finegd.empty()
@@ -372,7 +372,14 @@ class Calculation:
         t0 = time.perf_counter()
         self.update_hamiltonian()
         step = None
+        # a judged (learned) preconditioner: keep the state each iteration
+        # starts from, so that an iteration its failure has made non-finite
+        # can be taken back
+        snap = (_Snapshot(self) if getattr(self.preconditioner, 'failed', None)
+                is not None else None)
         for it in range(1, maxiter + 1):
+            if snap is not None:
+                snap.take()
             if graph and self.mixer.count == self.mixer.nmaxold:
                 if step is None:
                     step = _GraphedIteration(self)
@@ -388,6 +395,15 @@ class Calculation:
                 if step is not None:
                     step.release()
                     step = None
+                if not np.all(np.isfinite([E, err, ddens])):
+                    # the failed iteration produced NaN / inf: restart it
+                    # from the kept state with the multigrid
+                    snap.restore()
+                    snap = None
+                    log.times.append(time.perf_counter() - t0)
+                    log.iterations = it
+                    continue
+                snap = None
             log.energies.append(E)
             log.errors.append(err * Hartree**2 / self.nvalence)
             log.ddens.append(ddens)
@@ -436,6 +452,41 @@ def h2(vacuum=3.0, d=0.74):
     cell = [2 * vacuum, 2 * vacuum, 2 * vacuum + d]
     pos = np.array([[vacuum, vacuum, vacuum], [vacuum, vacuum, vacuum + d]])
     return ['H', 'H'], pos, cell
+
+
+class _Snapshot:
+    """The state an SCF iteration starts from (wave functions, projections,
+    eigenvalues, density), copied on the device before each iteration while
+    a judged preconditioner is in use.  `restore` puts it back, restarts the
+    density mixing and rebuilds the potential from the kept density."""
+
+    def __init__(self, calc):
+        self.calc = calc
+        self.kept = None
+
+    def take(self):
+        kpt = self.calc.wfs.kpt_u[0]
+        items = [kpt.psit_nG, kpt.P_nM, kpt.eps_n, self.calc.nt_G]
+        if self.kept is None or any(
+                (a is None) != (b is None) or (a is not None and a.shape != b.shape)
+                for a, b in zip(items, self.kept)):
+            self.kept = [None if a is None else torch.empty_like(a) for a in items]
+        for dst, src in zip(self.kept, items):
+            if src is not None:
+                dst.copy_(src)
+
+    def restore(self):
+        calc = self.calc
+        kpt = calc.wfs.kpt_u[0]
+        psit, P, eps, nt = self.kept
+        kpt.psit_nG.copy_(psit)
+        if P is not None:
+            kpt.P_nM.copy_(P)
+        if eps is not None:
+            kpt.eps_n = eps.clone()
+        calc.nt_G.copy_(nt)
+        calc.mixer.reset()
+        calc.update_hamiltonian()
 
 
 _POOL = None

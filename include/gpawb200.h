@@ -148,9 +148,13 @@ int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* rest1,
  * loads it); a call needing more -- about 1.41 x nin x level-0 points x
  * element size -- fails with GB_E_INVALID.  Nothing is allocated or freed.
  * The first call on a device looks up the array's address: make it before
- * any stream capture.  Calls share the array, so calls whose launches can
- * overlap on the GPU race: keep them on one stream.  Result in d0, as
- * gb_fd_precond. */
+ * any stream capture.  Under CUDA's lazy module loading (the default) that
+ * look-up is also what places the array in device memory, so a caller with
+ * a budget fixed at start-up makes one call then: nin = 0 does the look-up
+ * and launches nothing.  The address is kept per device and goes stale
+ * after cudaDeviceReset: do not call this entry point on that device again.
+ * Calls share the array, so calls whose launches can overlap on the GPU
+ * race: keep them on one stream.  Result in d0, as gb_fd_precond. */
 int gb_fd_precond_noalloc(const gb_transformer* rest0,
                           const gb_transformer* rest1,
                           const gb_transformer* intp1,
@@ -240,7 +244,8 @@ int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw,
  *           F: (2rh+1)^3, G: cc x 6^3 ([c][tx][ty][tz]); (rh, cc) in
  *           {(1, 1), (2, 16)}; xc (nb, cc, n/2) per axis; n2 >= 10;
  *           y must not overlap xf or xc (for (2, 16) the fine part is
- *           written first and the coarse part added by a second launch)
+ *           written first and the coarse part added by a second launch);
+ *           an overlapping y is refused with GB_E_INVALID
  *   stride: y[c][I] = sum_{|d|<=2} Q[d][c] x[2I + d], 16 channels out,
  *           Q [125][16], y (nb, 16, n/2) per axis */
 int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* xc,

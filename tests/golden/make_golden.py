@@ -1,9 +1,9 @@
 """Generate the golden vectors under tests/golden/ from the reference itself.
 
-Run in a container that has the reference source tree (REF, default
-/root/reference) and GPAW's C extension built from it by oracle/Makefile:
+Run where the reference source tree is present, with REF naming its root
+and GPAW's C extension built from it by oracle/Makefile:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<root> && REF=<root> python tests/golden/make_golden.py [sets]
 
 Outputs (committed; read by the CPU and GPU tests, which never need the
 reference tree at run time):
@@ -12,6 +12,9 @@ reference tree at run time):
   fd_kernels.npz outputs of _gpaw.Operator / Transformer / fd_precond on
                  seeded inputs (numpy default_rng(seed).standard_normal, so
                  inputs are regenerated from the seed, not stored)
+  xc.npz         _gpaw.XCFunctional outputs (LDA, PBE, revPBE, RPBE)
+  lfc.npz        _gpaw.spline_to_grid / LFC add, integrate, derivative
+  density.npz    _gpaw.add_to_density accumulations
 """
 from __future__ import annotations
 
@@ -24,7 +27,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = os.environ.get('REF', '/root/reference')
+REF = os.environ.get('REF')
+if not REF:
+    sys.exit('make_golden.py: set REF to the root of the reference source tree')
 sys.path.insert(0, str(REPO / 'oracle' / '_ref'))
 sys.path.insert(1, REF)
 sys.path.insert(2, str(REPO))
@@ -202,19 +207,6 @@ def xc_golden():
     return res
 
 
-def main():
-    np.savez_compressed(HERE / 'xc.npz', **xc_golden())
-    sten = stencils()
-    (HERE / 'stencils.json').write_text(json.dumps(sten))
-    res = kernels(sten)
-    np.savez_compressed(HERE / 'fd_kernels.npz', **res)
-    print(f'{len(sten)} stencils, {len(res)} kernel outputs')
-
-
-if __name__ == '__main__':
-    main()
-
-
 # ---------------------------------------------------------------- LFC
 from lfc_cases import LFC_CASES  # noqa: E402
 
@@ -291,5 +283,48 @@ def lfc_golden():
     return res
 
 
+# ---------------------------------------------------------------- density
+DENSITY_CASES = {
+    # name: (grid, bands, complex)
+    'real_4x31': ((31, 31, 31), 4, False),
+    'real_7x12x10x14': ((12, 10, 14), 7, False),
+    'complex_5x16': ((16, 16, 16), 5, True),
+}
+
+
+def density_golden():
+    """_gpaw.add_to_density (c/utilities.c:313-352) accumulated band by band
+    with occupations f_n = 2, 1.5, 1, ... as gpaw/wavefunctions/fd.py:95-100
+    calls it, on seeded wave functions (seed 3, regenerated by the tests)."""
+    res = {}
+    for name, (n_c, nb, cplx) in DENSITY_CASES.items():
+        rng = np.random.default_rng(3)
+        psit = rng.standard_normal((nb,) + n_c)
+        if cplx:
+            psit = psit + 1j * rng.standard_normal(psit.shape)
+        nt = np.full(n_c, 0.25)
+        f_n = 2.0 - 0.5 * np.arange(nb)
+        for f, psit_G in zip(f_n, psit):
+            _gpaw.add_to_density(float(f), np.ascontiguousarray(psit_G), nt)
+        res[name] = nt
+    return res
+
+
+def main(which):
+    if 'xc' in which:
+        np.savez_compressed(HERE / 'xc.npz', **xc_golden())
+    if 'kernels' in which:
+        sten = stencils()
+        (HERE / 'stencils.json').write_text(json.dumps(sten))
+        res = kernels(sten)
+        np.savez_compressed(HERE / 'fd_kernels.npz', **res)
+        print(f'{len(sten)} stencils, {len(res)} kernel outputs')
+    if 'lfc' in which:
+        np.savez_compressed(HERE / 'lfc.npz', **lfc_golden())
+    if 'density' in which:
+        np.savez_compressed(HERE / 'density.npz', **density_golden())
+
+
 if __name__ == '__main__':
-    np.savez_compressed(HERE / 'lfc.npz', **lfc_golden())
+    # python make_golden.py [xc] [kernels] [lfc] [density]  (default: all)
+    main(set(sys.argv[1:]) or {'xc', 'kernels', 'lfc', 'density'})

@@ -122,3 +122,22 @@ def test_product_path_fails_loudly_without_cuda_tensors():
     a = torch.zeros(tuple(gd.n_c), dtype=torch.float64)
     with pytest.raises(nat.GPAWB200Error):
         lap.apply(a, torch.zeros_like(a))
+
+
+def test_fold_fine_refuses_an_output_overlapping_its_inputs():
+    """The folded network's fine part writes y before its coarse part reads
+    xc and adds into y, so an aliased output is refused on the host, before
+    any launch (the check needs no GPU)."""
+    lib = nat.lib()
+    n_c = np.array([16, 16, 16], np.int64)
+    nb = 2
+    nf = nb * int(np.prod(n_c))
+    xf = np.zeros(nf, np.float32)
+    xc = np.zeros(nb * 16 * int(np.prod(n_c // 2)), np.float32)
+    F = np.zeros(125, np.float32)
+    G = np.zeros(16 * 216, np.float32)
+    p = lambda a, off=0: ctypes.c_void_p(a.ctypes.data + 4 * off)
+    for out in (p(xf), p(xf, nf // 2), p(xc, 100)):
+        rc = lib.gb_learned_fold_fine(p(xf), p(F), 2, p(xc), p(G), 16, out, nb,
+                                      nat.i64(n_c), None)
+        assert rc == -1 and b'overlaps' in lib.gb_last_error()

@@ -7,7 +7,9 @@ the library instead of from the caller.
 Checked through the C ABI against gb_fd_precond (the entry point whose work
 grids the caller allocates) on two calls in a row with different residuals,
 so that a second call cannot lean on what the first left in the shared
-array; and a request larger than the fixed array is refused with an error
+array; the second call must leave the device's free memory and torch's
+allocation count unchanged; a call with no grids does the one-time set-up
+only; and a request larger than the fixed array is refused with an error
 before anything is launched.  This file is collected last on purpose."""
 import numpy as np
 import pytest
@@ -57,6 +59,10 @@ def test_noalloc_matches_fd_precond(N, pbc, dtype):
         phases = np.exp(2j * np.pi * np.outer(k_c, [1, -1]))
     g = torch.Generator(device='cuda').manual_seed(11)
     real = torch.float64 if dtype == torch.complex128 else dtype
+    # set-up only: nothing to precondition, the array's address is looked up
+    nat.check(_noalloc(P, torch.empty(0, device='cuda', dtype=dtype),
+                       torch.empty(0, device='cuda', dtype=dtype), phases),
+              'gb_fd_precond_noalloc set-up')
     for call in range(2):
         shape = (5 + call,) + tuple(gd.n_c)
         res = torch.randn(shape, generator=g, device='cuda', dtype=real)
@@ -64,8 +70,15 @@ def test_noalloc_matches_fd_precond(N, pbc, dtype):
             res = torch.complex(res, torch.randn(shape, generator=g, device='cuda', dtype=real))
         want = P(res, _K(phases) if phases is not None else None)
         got = torch.full_like(res, float('nan'))
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        used0 = torch.cuda.memory_allocated()
         nat.check(_noalloc(P, res, got, phases), 'gb_fd_precond_noalloc')
         torch.cuda.synchronize()
+        if call == 1:
+            # the kernels are loaded by now: the call itself takes nothing
+            assert torch.cuda.mem_get_info()[0] == free0
+            assert torch.cuda.memory_allocated() == used0
         err = ((got - want).abs().max() / want.abs().max()).item()
         assert err < TOL[dtype], (call, err)
 
