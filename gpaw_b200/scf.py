@@ -20,12 +20,14 @@ gpaw/hamiltonian.py:232-282, 717-786), for norm-conserving HGH setups
 Precision modes: 'fp64' (everything FP64) and 'fp32' (wave functions,
 stencils, LFC, preconditioner and band GEMMs in FP32; Cholesky, eigh,
 Poisson, XC and every energy sum in FP64).
-Energies exclude the constant ion-ion term (irrelevant for convergence and
-for comparing precision modes of one geometry).
+Total energies have the zero of the reference's HGH setups: no atomic
+reference energy, the ion charges' self-energy removed, ion-ion
+interactions included through the Gaussian ion charges.
 """
 from __future__ import annotations
 
 import gc
+import itertools
 import time
 from dataclasses import dataclass, field
 
@@ -213,6 +215,7 @@ class Calculation:
         self.k_c = np.zeros(3) if k_c is None else np.asarray(k_c, float)
         self.vHt_g = self.finegd.zeros()
         self.dH_MM = None
+        self.e_constant = self._constant_energy()
         self._init_wavefunctions()
         self._init_density()
 
@@ -313,14 +316,46 @@ class Calculation:
         return dH.to(self.gd.device)
 
     def total_energy(self, kpt):
-        """E = sum f eps - int nt vt + E_H + E_xc + E_vbar (Hartree),
+        """E = sum f eps - int nt vt + E_H + E_xc + E_vbar + E_0 (Hartree),
         all sums in FP64 (the band energy counts kinetic + nonlocal +
-        local parts of the input potential)."""
+        local parts of the input potential); E_0 is the geometry constant
+        of `_constant_energy`."""
         if getattr(kpt, '_f_t', None) is None:
             kpt._f_t = torch.as_tensor(np.asarray(kpt.f_n, float), device=self.gd.device)
         band = (kpt._f_t * kpt.eps_n).sum()
         nvt = (self.nt_G * self.vt_G).sum() * self.gd.dv
-        return band - nvt + self.e_terms.sum()
+        return band - nvt + self.e_terms.sum() + self.e_constant
+
+    def _constant_energy(self):
+        """The energy zero of the reference's HGH setups.  The Hartree term
+        0.5 int rhot v_H contains each Gaussian ion charge's self-energy
+        Z^2 / (2 sqrt(pi) s), which the reference removes through the setup
+        constant M = -Eh_compcharge (gpaw/pseudopotential.py:293,
+        gpaw/hgh.py:171-174); and its Gaussian-Gaussian interactions are
+        those of widths s, where the reference's compensation charges have
+        width r_loc (gpaw/hgh.py:102, 249-258): the difference
+        sum_{a != b} Z_a Z_b [erf(R / w_loc) - erf(R / w_s)] / (2 R),
+        w = sqrt(2 (s_a^2 + s_b^2)), summed over the neighbouring periodic
+        images, is added.  No atomic reference energy is subtracted (the
+        reference's HGH setups have E = 0)."""
+        from scipy.special import erf
+        setups = self.setups
+        Z = np.array([s.Z for s in setups], float)
+        rl = np.array([s.rloc for s in setups])
+        sg = np.array([s.r_gauss for s in setups])
+        e = -(Z**2 / (2 * np.sqrt(np.pi) * sg)).sum()
+        pos_av = self.spos_ac @ self.cell_cv
+        w_loc = np.sqrt(2 * (rl[:, None]**2 + rl[None, :]**2))
+        w_s = np.sqrt(2 * (sg[:, None]**2 + sg[None, :]**2))
+        ZZ = Z[:, None] * Z[None, :]
+        shifts = [(-1, 0, 1) if p else (0,) for p in self.pbc]
+        for n_c in itertools.product(*shifts):
+            d = pos_av[None, :, :] + np.dot(n_c, self.cell_cv) - pos_av[:, None, :]
+            R = np.linalg.norm(d, axis=2)
+            if not any(n_c):
+                np.fill_diagonal(R, np.inf)
+            e += 0.5 * (ZZ * (erf(R / w_loc) - erf(R / w_s)) / R).sum()
+        return float(e)
 
     def update_density(self):
         nt_out = self.gd.zeros()
