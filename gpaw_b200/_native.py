@@ -93,6 +93,13 @@ _SIGNATURES = {
                                c_void_p, c_void_p]),
     'gb_band_combine': (c_int, [c_int64, c_int64, c_int, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_int64, c_int, c_void_p]),
+    'gb_spline_new': (c_int, [c_int, c_double, c_int, PD, POINTER(c_void_p)]),
+    'gb_spline_free': (c_int, [c_void_p]),
+    'gb_spline_get': (c_int, [c_void_p, POINTER(c_int), PD, POINTER(c_int)]),
+    'gb_spline_to_grid': (c_int, [c_void_p, P64, P64, PD, PD, P64, P64, c_void_p,
+                                  c_void_p, P64, P64, c_void_p]),
+    'gb_lfc_derivative': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, PD, P64,
+                                  POINTER(c_void_p), P64, PD, c_int, c_int, c_void_p]),
     'gb_xc_calculate': (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_void_p, c_void_p]),
     'gb_fd_precond': (c_int, [c_void_p] * 7 + [c_void_p] * 8 +

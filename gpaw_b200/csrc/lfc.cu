@@ -15,14 +15,18 @@
 //    reduces dv * phase_W * sum_G a[x][G] A_W[row][m] over every image and
 //    adds the block's result to c[x][M..M+nm) -- again a single writer.
 //
-// Derivatives (forces) use the same integrate kernel on a second object whose
-// rows hold the 3*nm Cartesian derivatives (layout [m][v], c_xMv).
+// Derivatives (gb_lfc_derivative, c/lfc.c:1449-1601) are computed on the
+// fly from the radial splines: one CTA per (function group, band) walks the
+// group's rows, evaluates d/dr_v [f(r) r^l Y_lm] at each point (spline value
+// and slope, solid harmonics and their gradients) and reduces
+// dv sum_G a[x][G] phase_W d/dr_v Phi to c[x][M][v] -- a single writer.
 #include <algorithm>
 #include <cstring>
 #include <map>
 #include <type_traits>
 #include <vector>
 #include "internal.cuh"
+#include "spline.cuh"
 
 struct gb_lfc {
   int nW = 0, nM = 0, maxnm = 0;
@@ -87,6 +91,13 @@ struct LfcView {
   const int64_t* vol_row1;
   const int* row_G;
   const int64_t* vol_aoff;
+};
+
+// grid geometry for on-the-fly positions (h_cv row-major, local sizes, and
+// the global index of the local grid's first point)
+struct DerivGeom {
+  double h[9];
+  int64_t n[3], beg[3];
 };
 
 static LfcView view(const gb_lfc* l) {
@@ -558,6 +569,130 @@ static __global__ void to_float(const double* a, float* b, int64_t n) {
 
 }  // namespace gb
 
+namespace gb {
+SplineDev spline_view(const gb_spline* s);
+
+struct SplineM {          // the radial function of one M and its m index
+  SplineDev s;
+  int m;
+};
+
+// one CTA per (function group, band); up to 16 functions per volume
+template <typename T>
+__global__ void __launch_bounds__(128) lfc_derivative_kernel(const LfcView l, const SplineM* __restrict__ spl,
+                                                             const double* __restrict__ pos_W, DerivGeom geo,
+                                                             const T* __restrict__ a_xG, T* __restrict__ c_xMv,
+                                                             int q) {
+  constexpr bool CPLX = Elem<T>::cplx;
+  using Acc = typename std::conditional<CPLX, double2, double>::type;
+  constexpr int NT = 128, NMV = 48;
+  __shared__ Acc red[NT / 32][NMV];
+  const int g = blockIdx.x;
+  const int64_t x = blockIdx.y;
+  const int M0 = l.gr_M[g];
+  const int nm = l.gr_nm[g];
+  Acc acc[NMV];
+#pragma unroll
+  for (int i = 0; i < NMV; ++i) acc[i] = zero<Acc>();
+  for (int vi = l.gr_voff[g]; vi < l.gr_voff[g + 1]; ++vi) {
+    const int W = l.gv_W[vi];
+    double pr = 1.0, pi = 0.0;
+    if (CPLX && q >= 0) {
+      const double2 ph = l.phase[(int64_t)q * l.nW + W];
+      pr = ph.x;
+      pi = ph.y;
+    }
+    const double px = pos_W[3 * W], py = pos_W[3 * W + 1], pz = pos_W[3 * W + 2];
+    for (int64_t r = l.vol_row0[W] + threadIdx.x; r < l.vol_row1[W]; r += NT) {
+      const int64_t G = l.row_G[r];
+      const int64_t i2 = G % geo.n[2] + geo.beg[2];
+      const int64_t i1 = (G / geo.n[2]) % geo.n[1] + geo.beg[1];
+      const int64_t i0 = G / (geo.n[2] * geo.n[1]) + geo.beg[0];
+      const double X = geo.h[0] * i0 + geo.h[3] * i1 + geo.h[6] * i2 - px;
+      const double Y = geo.h[1] * i0 + geo.h[4] * i1 + geo.h[7] * i2 - py;
+      const double Z = geo.h[2] * i0 + geo.h[5] * i1 + geo.h[8] * i2 - pz;
+      const double r2 = X * X + Y * Y + Z * Z;
+      const double rr = sqrt(r2);
+      Acc av;
+      if constexpr (CPLX) {
+        const T v = a_xG[x * l.nG + G];
+        av = make_double2((double)v.x * pr - (double)v.y * pi, (double)v.x * pi + (double)v.y * pr);
+      } else {
+        av = (double)a_xG[x * l.nG + G];
+      }
+      // per function: f, df/dr once, then every m
+      const double* coef_prev = nullptr;
+      double f = 0.0, df = 0.0;
+      double Yl[5], dY[15];
+      for (int k = 0; k < nm && k < 16; ++k) {
+        const SplineM sm = spl[M0 + k];
+        if (sm.s.coef != coef_prev || sm.m == 0) {
+          spline_eval(sm.s, rr, f, df);
+          const double fr = rr > 1e-15 ? df / rr : 0.0;
+          solid_harmonics(sm.s.l, fr, X, Y, Z, r2, Yl);        // (df/dr / r) r^l Y_lm
+          solid_harmonics_gradient(sm.s.l, f, X, Y, Z, dY);    // f d(r^l Y_lm)/dr_v
+          coef_prev = sm.s.coef;
+        }
+        const double d0 = dY[3 * sm.m] + Yl[sm.m] * X;
+        const double d1 = dY[3 * sm.m + 1] + Yl[sm.m] * Y;
+        const double d2 = dY[3 * sm.m + 2] + Yl[sm.m] * Z;
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk)
+          if (kk == k) {
+            if constexpr (CPLX) {
+              acc[3 * kk] = make_double2(acc[3 * kk].x + av.x * d0, acc[3 * kk].y + av.y * d0);
+              acc[3 * kk + 1] = make_double2(acc[3 * kk + 1].x + av.x * d1, acc[3 * kk + 1].y + av.y * d1);
+              acc[3 * kk + 2] = make_double2(acc[3 * kk + 2].x + av.x * d2, acc[3 * kk + 2].y + av.y * d2);
+            } else {
+              acc[3 * kk] += av * d0;
+              acc[3 * kk + 1] += av * d1;
+              acc[3 * kk + 2] += av * d2;
+            }
+          }
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NMV; ++i) {
+    Acc v = acc[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      if constexpr (CPLX) {
+        v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+      } else {
+        v += __shfl_down_sync(0xffffffffu, v, o);
+      }
+    }
+    if (lane == 0) red[warp][i] = v;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 3 * nm && e < NMV; e += NT) {
+    Acc v = zero<Acc>();
+    for (int w = 0; w < NT / 32; ++w) v = add(v, red[w][e]);
+    T* cp = c_xMv + (x * l.nM + M0) * 3 + e;
+    if constexpr (CPLX) {
+      cp->x += (typename Elem<T>::R)(v.x * l.dv);
+      cp->y += (typename Elem<T>::R)(v.y * l.dv);
+    } else {
+      *cp += (T)(v * l.dv);
+    }
+  }
+}
+
+template <typename T>
+static int derivative_t(const gb_lfc* l, const SplineM* spl, const double* pos, const DerivGeom& geo,
+                        const void* a, void* c, int64_t nx, int q, cudaStream_t st) {
+  if (l->ngroups == 0) return GB_OK;
+  const dim3 grid((unsigned)l->ngroups, (unsigned)nx);
+  lfc_derivative_kernel<T><<<grid, 128, 0, st>>>(view(l), spl, pos, geo, static_cast<const T*>(a),
+                                                 static_cast<T*>(c), q);
+  return check_launch("lfc_derivative_kernel");
+}
+
+}  // namespace gb
+
 using namespace gb;
 
 extern "C" {
@@ -746,6 +881,60 @@ int gb_lfc_integrate(const gb_lfc* l, const void* a_xG, void* c_xM, int64_t nx, 
     case GB_DTYPE_C128: return integrate_t<double2>(l, a_xG, c_xM, nx, q, st);
     default: return integrate_t<float2>(l, a_xG, c_xM, nx, q, st);
   }
+}
+
+int gb_lfc_derivative(const gb_lfc* l, const void* a_xG, void* c_xMv, int64_t nx, const double h_cv[9],
+                      const int64_t n_c[3], const gb_spline* const* spline_M, const int64_t beg_c[3],
+                      const double* pos_Wv, int q, int dtype, void* stream) {
+  GB_REQUIRE(l && dtype_valid(dtype) && nx >= 0, "gb_lfc_derivative: bad arguments");
+  if (nx == 0 || l->nM == 0) return GB_OK;
+  GB_REQUIRE(a_xG && c_xMv && h_cv && n_c && beg_c && pos_Wv && spline_M, "gb_lfc_derivative: null argument");
+  GB_REQUIRE(q < l->nq, "gb_lfc_derivative: k-point index out of range");
+  GB_REQUIRE(nx < 65536, "gb_lfc_derivative: at most 65535 grids per call");
+  GB_REQUIRE(n_c[0] * n_c[1] * n_c[2] == l->nG, "gb_lfc_derivative: grid size does not match the object");
+  for (int g = 0; g < l->ngroups; ++g)
+    if (l->h_gr_nm[g] > 16) return fail(GB_E_UNSUPPORTED, "gb_lfc_derivative: more than 16 functions in a volume");
+  // per M: the spline and its m index (m runs 0 .. 2l across consecutive
+  // entries of one function, as the reference's spline_M list repeats each
+  // function's spline 2l + 1 times)
+  std::vector<SplineM> hs(l->nM);
+  for (int M = 0; M < l->nM; ++M) {
+    const gb_spline* sp = spline_M[M];
+    if (!sp) return fail(GB_E_INVALID, "gb_lfc_derivative: null spline in spline_M");
+    const int nmf = 2 * sp->l + 1;
+    int m = 0;
+    if (M > 0 && spline_M[M - 1] == sp && hs[M - 1].m + 1 < nmf) m = hs[M - 1].m + 1;
+    hs[M] = SplineM{spline_view(sp), m};
+  }
+  DerivGeom geo;
+  for (int c = 0; c < 3; ++c) {
+    geo.n[c] = n_c[c];
+    geo.beg[c] = beg_c[c];
+  }
+  for (int i = 0; i < 9; ++i) geo.h[i] = h_cv[i];
+  cudaStream_t st = (cudaStream_t)stream;
+  void* work = nullptr;
+  const size_t sbytes = hs.size() * sizeof(SplineM), pbytes = (size_t)l->nW * 3 * sizeof(double);
+  if (cudaMallocAsync(&work, sbytes + pbytes + 16, st) != cudaSuccess)
+    return fail(GB_E_NOMEM, "gb_lfc_derivative: work space allocation failed");
+  SplineM* d_spl = static_cast<SplineM*>(work);
+  double* d_pos = reinterpret_cast<double*>(static_cast<char*>(work) + (sbytes + 15) / 16 * 16);
+  int rc = GB_OK;
+  if (cudaMemcpyAsync(d_spl, hs.data(), sbytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d_pos, pos_Wv, pbytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    rc = fail(GB_E_CUDA, "gb_lfc_derivative: upload failed");
+  if (!rc) {
+    switch (dtype) {
+      case GB_DTYPE_F64: rc = derivative_t<double>(l, d_spl, d_pos, geo, a_xG, c_xMv, nx, -1, st); break;
+      case GB_DTYPE_F32: rc = derivative_t<float>(l, d_spl, d_pos, geo, a_xG, c_xMv, nx, -1, st); break;
+      case GB_DTYPE_C128: rc = derivative_t<double2>(l, d_spl, d_pos, geo, a_xG, c_xMv, nx, q, st); break;
+      default: rc = derivative_t<float2>(l, d_spl, d_pos, geo, a_xG, c_xMv, nx, q, st); break;
+    }
+  }
+  cudaFreeAsync(work, st);
+  // the host vectors above were read by the copies: finish them before return
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = fail(GB_E_CUDA, "gb_lfc_derivative: sync failed");
+  return rc;
 }
 
 }  // extern "C"

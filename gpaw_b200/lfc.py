@@ -6,13 +6,15 @@ forces)`` with ``set_positions``, ``add``, ``integrate``, ``derivative``,
 keyed by atom index (``c_axi[a]`` of shape xshape + (ni,)), grids are CUDA
 tensors (..., n0, n1, n2).
 
-When positions change, the host tabulates every atom-centred function
-f_j(|r - R|) r^l Y_lm on the grid points of its boxes (the values
-spline_to_grid produces, c/lfc.c:887-977, with the same box rule
-gpaw/grid_descriptor.py:344-411 and the same point order), sorts the
-boundary events (gpaw/lfc.py:259-374) and hands them to gb_lfc_new, which
-builds the device indices once.  add / integrate / derivative are then one
-or a few kernel launches for all bands.
+When positions change, every atom-centred function f_j(|r - R|) r^l Y_lm
+is tabulated on the grid points of its boxes by the device spline_to_grid
+(gb_spline_to_grid, c/lfc.c:887-977; boxes by the rule of
+gpaw/grid_descriptor.py:344-411), the boundary events are sorted
+(gpaw/lfc.py:259-374) and handed to gb_lfc_new, which builds the device
+indices once.  add / integrate / derivative are then one or a few kernel
+launches for all bands; the derivative evaluates the splines' slopes on the
+device (gb_lfc_derivative).  Grid descriptors on the CPU (host-side set-up
+checks only) tabulate with numpy instead.
 """
 from __future__ import annotations
 
@@ -22,34 +24,52 @@ import numpy as np
 import torch
 
 from gpaw_b200 import _native as nat
-from gpaw_b200.spline import rlYlm, rlYlm_gradient
+from gpaw_b200.spline import rlYlm
 
 
-def _box_functions(spline, beg_c, end_c, pos_v, gd, derivative=False):
+def spline_to_grid(spline, beg_c, end_c, pos_v, h_cv, n_c, gdcorner_c, device='cuda'):
+    """_gpaw.spline_to_grid on the device: (A_gm, G_B) -- f(r) r^l Y_lm at
+    the box points with r < rmax as a CUDA tensor (ng, 2l + 1), rows (g0, g1)
+    in order and g2 increasing, and the [start, end) runs of those points
+    in the local grid's flat index (int32 numpy array)."""
+    beg_c = np.asarray(beg_c, np.int64)
+    end_c = np.asarray(end_c, np.int64)
+    ext = np.maximum(end_c - beg_c, 0)
+    nm = 2 * spline.l + 1
+    npts = int(np.prod(ext))
+    A = torch.empty((max(npts, 1), nm), dtype=torch.float64, device=device)
+    G = torch.empty(max(2 * int(ext[0] * ext[1]), 2), dtype=torch.int32, device=device)
+    ng = ctypes.c_int64()
+    nB = ctypes.c_int64()
+    nat.check(nat.lib().gb_spline_to_grid(
+        spline.handle, nat.i64(beg_c), nat.i64(end_c), nat.f64(pos_v),
+        nat.f64(np.ascontiguousarray(h_cv)), nat.i64(n_c), nat.i64(gdcorner_c),
+        nat.ptr(A), nat.ptr(G), ctypes.byref(ng), ctypes.byref(nB),
+        nat.stream_of(A)), 'gb_spline_to_grid')
+    return A[:ng.value], G[:nB.value].cpu().numpy()
+
+
+def _box_functions(spline, beg_c, end_c, pos_v, gd):
     """Values of one radial function on one box: (A_gm, G_b) as
-    spline_to_grid returns them (rows in g0, g1, g2 order, runs along g2),
-    or the (ng, nm, 3) Cartesian derivatives when `derivative`."""
+    spline_to_grid returns them (rows in g0, g1, g2 order, runs along g2).
+    On a CUDA grid descriptor the values come from the device
+    spline_to_grid; on a CPU one (host-side set-up checks) from numpy."""
+    if torch.device(gd.device).type == 'cuda':
+        A, G_b = spline_to_grid(spline, beg_c, end_c, pos_v, gd.h_cv, gd.n_c,
+                                gd.beg_c, gd.device)
+        return A.cpu().numpy(), G_b
     l = spline.l
     rcut = spline.rmax
     g = np.indices(tuple(end_c - beg_c)).reshape(3, -1).T + beg_c
     d = g @ gd.h_cv - pos_v
-    r2 = (d**2).sum(1)
-    r = np.sqrt(r2)
+    r = np.sqrt((d**2).sum(1))
     inside = r < rcut
     g = g[inside]
     d = d[inside]
     r = r[inside]
-    f, df = spline.value_and_derivative(r)
+    f, _ = spline.value_and_derivative(r)
     x, y, z = d.T
-    Y = rlYlm(l, x, y, z)                       # (nm, ng)
-    if derivative:
-        dY = rlYlm_gradient(l, x, y, z)         # (nm, 3, ng)
-        with np.errstate(divide='ignore', invalid='ignore'):
-            fr = np.where(r > 1e-15, df / r, 0.0)
-        A = f[None, None] * dY + (fr * Y)[:, None] * d.T[None]
-        A = np.ascontiguousarray(A.transpose(2, 0, 1))   # (ng, nm, 3)
-    else:
-        A = np.ascontiguousarray((f * Y).T)             # (ng, nm)
+    A = np.ascontiguousarray((f * rlYlm(l, x, y, z)).T)    # (ng, nm)
     # flat local index and z-runs
     rel = g - gd.beg_c
     G = (rel[:, 0] * gd.n_c[1] + rel[:, 1]) * gd.n_c[2] + rel[:, 2]
@@ -359,37 +379,44 @@ class LocalizedFunctionsCollection(BaseLFC):
                 c_axi[a][:] = c_xM[..., M1:M1 + self.sphere_a[a].Mmax]
         return c_xM
 
-    def _derivative_object(self):
+    def _derivative_arguments(self):
+        """The reference's arguments of LFC.derivative for this object:
+        one spline per M (each function's repeated 2l + 1 times) and the
+        centre of every device volume (its atom's periodic image)."""
         if self._deriv is None:
-            dA_W = []
-            for (a, ng, members) in self.box_W:
-                sphere = self.sphere_a[a]
-                dA = np.zeros((ng, 3 * sphere.Mmax))
-                for (j, beg_c, end_c, pos_v), rows, Mw in members:
-                    spline = sphere.spline_j[j]
-                    d, _ = _box_functions(spline, beg_c, end_c, pos_v, self.gd,
-                                          derivative=True)
-                    dA[rows, 3 * Mw:3 * Mw + d.shape[1] * 3] = d.reshape(d.shape[0], -1)
-                dA_W.append(dA)
-            nG = int(np.prod(self.gd.n_c))
-            self._deriv = _Native(dA_W, 3 * self.M_W, self.G_B, self.W_B,
-                                  self.gd.dv, self.phase_qW, nG, 3 * self.Mmax)
+            spline_M = []
+            for sphere in self.sphere_a:
+                for spline in sphere.spline_j:
+                    spline_M.extend([spline] * (2 * spline.l + 1))
+            spos_a = [sphere.spos_c for sphere in self.sphere_a]
+            pos_Wv = np.array([np.dot(spos_a[a] - sd, self.gd.cell_cv)
+                               for (a, _, _), sd in zip(self.box_W, self.sdisp_Wc)])
+            self._deriv = (spline_M, np.ascontiguousarray(pos_Wv.reshape(-1, 3), float))
         return self._deriv
 
     def derivative(self, a_xG, c_axiv, q=-1):
         """c_axiv = dv sum_G a_xG dPhi^a_i*/dv (gpaw/lfc.py:633-724);
-        d/dR = -d/dr is left to the caller exactly as in the reference."""
+        d/dR = -d/dr is left to the caller exactly as in the reference.
+        Computed on the device from the splines' values and slopes
+        (gb_lfc_derivative); functions normalised to a given integral
+        (integral=...) are refused, as their derivative needs the chain
+        rule of the normalisation."""
         if self.integral_a is not None:
             raise NotImplementedError('derivative of normalized functions')
         nat.require_cuda(a_xG)
-        d = self._derivative_object()
         xshape = tuple(a_xG.shape[:-3])
-        c_xMv = torch.zeros(xshape + (3 * self.Mmax,), dtype=a_xG.dtype, device=a_xG.device)
+        c_xMv = torch.zeros(xshape + (self.Mmax, 3), dtype=a_xG.dtype, device=a_xG.device)
         nx = int(np.prod(xshape, dtype=np.int64))
-        nat.check(nat.lib().gb_lfc_integrate(
-            d.handle, nat.ptr(a_xG), nat.ptr(c_xMv), nx, nat.dtype_code(a_xG),
-            self._nq(a_xG, q), nat.stream_of(a_xG)), 'gb_lfc_integrate(derivative)')
-        c_xMv = c_xMv.reshape(xshape + (self.Mmax, 3))
+        if self.Mmax == 0 or nx == 0:
+            return c_xMv
+        spline_M, pos_Wv = self._derivative_arguments()
+        handles = (ctypes.c_void_p * len(spline_M))(*[sp.handle.value for sp in spline_M])
+        gd = self.gd
+        nat.check(nat.lib().gb_lfc_derivative(
+            self.lfc.handle, nat.ptr(a_xG), nat.ptr(c_xMv), nx,
+            nat.f64(np.ascontiguousarray(gd.h_cv)), nat.i64(gd.n_c), handles,
+            nat.i64(gd.beg_c), nat.f64(pos_Wv), self._nq(a_xG, q),
+            nat.dtype_code(a_xG), nat.stream_of(a_xG)), 'gb_lfc_derivative')
         for a in self.my_atom_indices:
             if a in c_axiv:
                 M1 = self.M_a[a]

@@ -56,6 +56,30 @@ class Spline:
         s[:nbins, 3] = (f2[1:] - f2[:-1]) / (6 * dr)
         return s
 
+    # -- device object ----------------------------------------------------
+    @property
+    def handle(self):
+        """The gb_spline of this function (made on first use; holds the
+        coefficient table in device memory)."""
+        h = getattr(self, '_handle', None)
+        if h is None:
+            from gpaw_b200 import _native as nat
+            h = nat.c_void_p()
+            nat.check(nat.lib().gb_spline_new(self.l, self.rmax, self.nbins,
+                                              nat.f64(self.f_g), nat.ctypes.byref(h)),
+                      'gb_spline_new')
+            self._handle = h
+        return h
+
+    def __del__(self):
+        h = getattr(self, '_handle', None)
+        if h is not None and h.value:
+            try:
+                from gpaw_b200 import _native as nat
+                nat.lib().gb_spline_free(h)
+            except Exception:
+                pass
+
     # -- reference interface ----------------------------------------------
     def get_cutoff(self):
         return self.rmax
@@ -116,23 +140,4 @@ def rlYlm(l, x, y, z):
         r2 = x * x + y * y + z * z
         return np.array([_C2A * x * y, _C2A * y * z, _C20 * (3 * z * z - r2),
                          _C2A * x * z, _C22 * (x * x - y * y)])
-    raise NotImplementedError('l > 2 localized functions')
-
-
-def rlYlm_gradient(l, x, y, z):
-    """(2l+1, 3, ...) array of d(r^l Y_lm)/d(x, y, z)."""
-    zero = np.zeros_like(x)
-    one = np.ones_like(x)
-    if l == 0:
-        return np.array([[zero, zero, zero]])
-    if l == 1:
-        return _C1 * np.array([[zero, one, zero], [zero, zero, one],
-                               [one, zero, zero]])
-    if l == 2:
-        return np.array([
-            [_C2A * y, _C2A * x, zero],
-            [zero, _C2A * z, _C2A * y],
-            [_C20 * -2 * x, _C20 * -2 * y, _C20 * 4 * z],
-            [_C2A * z, zero, _C2A * x],
-            [_C22 * 2 * x, _C22 * -2 * y, zero]])
     raise NotImplementedError('l > 2 localized functions')

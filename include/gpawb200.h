@@ -165,6 +165,35 @@ int gb_fd_precond_noalloc(const gb_transformer* rest0,
                           int dtype, const double* phase_cd, void* stream);
 
 /* ======================================================================
+ * Radial splines and spline_to_grid  -- replace _gpaw.Spline and
+ * _gpaw.spline_to_grid
+ *   reference: c/spline.c (NewSplineObject), c/bmgs/spline.c:11-75
+ *              (natural cubic spline, value and slope), c/lfc.c:887-977
+ *              (spline_to_grid), c/bmgs/spherical_harmonics.h:5-48
+ *   called from gpaw/spline.py:19-31 and gpaw/lfc.py:94-97 (Sphere)
+ * gb_spline_new: f_g holds nbins + 1 host values on r = 0 .. rmax (the
+ *   last one is taken as given; Spline.from_data zeroes it); l <= 2.
+ * gb_spline_to_grid: f(r) r^l Y_lm on the box beg_c <= g < end_c (global
+ *   grid indices) around pos_v (Bohr), h_cv row-major, n_c the local grid
+ *   and gdcorner_c its first global index.  Device outputs: A_gm rows for
+ *   every point with r < rmax, rows (g0, g1) in order and g2 increasing
+ *   within each (capacity: box points x (2l + 1) doubles), and G_B the
+ *   [start, end) flat local indices of the runs along g2 (capacity: 2 x box
+ *   rows ints).  *ng_out points and *nB_out entries of G_B are written
+ *   back (the call waits for its stream).
+ * ==================================================================== */
+typedef struct gb_spline gb_spline;
+int gb_spline_new(int l, double rmax, int nbins, const double* f_g,
+                  gb_spline** out);
+int gb_spline_free(gb_spline* s);
+int gb_spline_get(const gb_spline* s, int* l, double* rmax, int* nbins);
+int gb_spline_to_grid(const gb_spline* s, const int64_t beg_c[3],
+                      const int64_t end_c[3], const double pos_v[3],
+                      const double h_cv[9], const int64_t n_c[3],
+                      const int64_t gdcorner_c[3], double* A_gm, int* G_B,
+                      int64_t* ng_out, int64_t* nB_out, void* stream);
+
+/* ======================================================================
  * Localized functions (LFC)  -- replaces _gpaw.LFC
  *   reference: c/lfc.c:146-257 (NewLFCObject), c/lfc.c:818-885 (add),
  *              c/lfc.c:432-505 (integrate), c/lfc.h:79-130 (GRID_LOOP),
@@ -190,6 +219,19 @@ int gb_lfc_add(const gb_lfc* lfc, const void* c_xM, void* a_xG, int64_t nx,
 int gb_lfc_integrate(const gb_lfc* lfc, const void* a_xG, void* c_xM,
                      int64_t nx, int dtype, int q, void* stream);
 int gb_lfc_free(gb_lfc* lfc);
+/* LFC.derivative (c/lfc.c:1449-1601, called from gpaw/lfc.py:680-682):
+ *   c_xMv[x][M][v] += dv sum_G a_xG[x][G] phase_qW d/dr_v Phi_M(r_G - R_W)
+ * computed on the fly from the radial splines; arguments as the
+ * reference's: h_cv row-major, n_c / beg_c the local grid and its first
+ * global index, spline_M one spline per M (each function's spline
+ * repeated 2l + 1 times), pos_Wv the centre of every volume the object was
+ * built with (nW x 3, Bohr), q the k-point (-1 for real data).  Volumes of
+ * at most 16 functions; c_xMv (nx, nM, 3) accumulates like integrate.
+ * d/dR = -d/dr is left to the caller, as in the reference. */
+int gb_lfc_derivative(const gb_lfc* lfc, const void* a_xG, void* c_xMv,
+                      int64_t nx, const double h_cv[9], const int64_t n_c[3],
+                      const gb_spline* const* spline_M, const int64_t beg_c[3],
+                      const double* pos_Wv, int q, int dtype, void* stream);
 
 /* ======================================================================
  * Exchange-correlation on the grid  -- replaces _gpaw.XCFunctional.calculate

@@ -284,6 +284,25 @@ class PulayMixer:
 
 
 # ---------------------------------------------------------------- SCF
+def setup_data(s):
+    """The plain radial data of a setup object with the attributes Z,
+    rloc, r_gauss, vbar / ghat / nguess splines, pt_j and dH_ii (splines
+    with l, rmax, f_g)."""
+    sp = lambda x: (x.l, x.rmax, np.array(x.f_g))
+    return dict(Z=s.Z, rloc=s.rloc, r_gauss=s.r_gauss, vbar=sp(s.vbar),
+                ghat=sp(s.ghat), nguess=sp(s.nguess),
+                pt=[sp(p) for p in s.pt_j], dH=np.asarray(s.dH_ii, float))
+
+
+def from_calculation(calc, **kwargs):
+    """The oracle on a device calculation's geometry, setups, occupations
+    and start (its current wave functions, widened to FP64)."""
+    kpt = calc.wfs.kpt_u[0]
+    return SCF([setup_data(s) for s in calc.setups], calc.spos_ac, calc.cell_cv,
+               calc.pbc, calc.gd.N_c, kpt.psit_nG.double().cpu().numpy(),
+               np.asarray(kpt.f_n), mixer_beta=calc.mixer.beta, **kwargs)
+
+
 def h2gpts(h, cell_cv, idiv=4):
     """gpaw/utilities/__init__.py:108-120."""
     L_c = (np.linalg.inv(cell_cv)**2).sum(0)**-0.5

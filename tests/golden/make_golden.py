@@ -15,6 +15,7 @@ reference tree at run time):
   xc.npz         _gpaw.XCFunctional outputs (LDA, PBE, revPBE, RPBE)
   lfc.npz        _gpaw.spline_to_grid / LFC add, integrate, derivative
   density.npz    _gpaw.add_to_density accumulations
+  spline_to_grid.npz  _gpaw.spline_to_grid tables and runs, box by box
 """
 from __future__ import annotations
 
@@ -310,6 +311,41 @@ def density_golden():
     return res
 
 
+# ---------------------------------------------------------------- splines
+SPLINE_CASES = {
+    # name: (N_c, cell_cv (Bohr), pbc, spos_c, l, rmax, nbins)
+    'zero_l0': ((20, 22, 24), np.diag([5.0, 5.5, 6.0]), (0, 0, 0), (0.5, 0.45, 0.52), 0, 2.3, 40),
+    'periodic_l1': ((20, 20, 24), np.diag([5.0, 5.0, 6.0]), (1, 1, 1), (0.05, 0.9, 0.5), 1, 2.6, 52),
+    'mixed_l2': ((18, 20, 22), np.diag([4.5, 5.0, 5.5]), (0, 1, 1), (0.3, 0.02, 0.97), 2, 2.2, 30),
+    'fcc_l2': ((16, 16, 16), np.array([[0, 3.4, 3.4], [3.4, 0, 3.4], [3.4, 3.4, 0]]),
+               (1, 1, 1), (0.1, 0.3, 0.6), 2, 2.0, 25),
+}
+
+
+def spline_radial(rmax, nbins):
+    f = np.exp(-(np.linspace(0, rmax, nbins + 1) / (0.4 * rmax))**2)
+    f[-1] = 0.0
+    return f
+
+
+def spline_golden():
+    """_gpaw.spline_to_grid (c/lfc.c:887-977) on every box
+    (gpaw/grid_descriptor.py:344-411) of one atom per case."""
+    sys.path.insert(0, str(REPO))
+    from oracle.scf import Grid, boxes
+    res = {}
+    for name, (N_c, cell_cv, pbc, spos, l, rmax, nbins) in SPLINE_CASES.items():
+        g = Grid(N_c, cell_cv, pbc)
+        s = _gpaw.Spline(l, rmax, spline_radial(rmax, nbins))
+        for i, (beg, end, sdisp) in enumerate(boxes(g, np.array(spos), rmax)):
+            pos_v = (np.array(spos) - sdisp) @ g.cell_cv
+            A_gm, G_b = _gpaw.spline_to_grid(s, beg, end, pos_v, np.ascontiguousarray(g.h_cv),
+                                             g.n_c, g.beg_c)
+            res[f'{name}|{i}|A'] = A_gm
+            res[f'{name}|{i}|G'] = G_b
+    return res
+
+
 def main(which):
     if 'xc' in which:
         np.savez_compressed(HERE / 'xc.npz', **xc_golden())
@@ -323,8 +359,10 @@ def main(which):
         np.savez_compressed(HERE / 'lfc.npz', **lfc_golden())
     if 'density' in which:
         np.savez_compressed(HERE / 'density.npz', **density_golden())
+    if 'spline' in which:
+        np.savez_compressed(HERE / 'spline_to_grid.npz', **spline_golden())
 
 
 if __name__ == '__main__':
-    # python make_golden.py [xc] [kernels] [lfc] [density]  (default: all)
-    main(set(sys.argv[1:]) or {'xc', 'kernels', 'lfc', 'density'})
+    # python make_golden.py [xc] [kernels] [lfc] [density] [spline]  (default: all)
+    main(set(sys.argv[1:]) or {'xc', 'kernels', 'lfc', 'density', 'spline'})

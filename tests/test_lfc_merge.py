@@ -50,29 +50,24 @@ def dense(rec, q=None):
     return Phi
 
 
-def dense_reference(gd, lfc, spos, q=None, derivative=False):
+def dense_reference(gd, lfc, spos, q=None):
     """The same matrix from the per-radial-function boxes directly."""
     from gpaw_b200.lfc import _box_functions
-    nM = lfc.Mmax * (3 if derivative else 1)
-    Phi = np.zeros((int(np.prod(gd.n_c)), nM), complex)
+    Phi = np.zeros((int(np.prod(gd.n_c)), lfc.Mmax), complex)
     for a, sphere in enumerate(lfc.sphere_a):
         M = 0
         for j, spline in enumerate(sphere.spline_j):
             nm = 2 * spline.l + 1
             for beg_c, end_c, sdisp_c in gd.get_boxes(spos[a], spline.rmax, lfc.cut):
                 pos_v = np.dot(spos[a] - sdisp_c, gd.cell_cv)
-                A, G_b = _box_functions(spline, beg_c, end_c, pos_v, gd, derivative)
+                A, G_b = _box_functions(spline, beg_c, end_c, pos_v, gd)
                 if len(G_b) == 0:
                     continue
                 G = np.concatenate([np.arange(g0, g1) for g0, g1 in zip(G_b[0::2], G_b[1::2])])
                 ph = (np.exp(2j * np.pi * np.dot(lfc.ibzk_qc[q], sdisp_c))
                       if q is not None else 1.0)
-                if derivative:
-                    c0 = 3 * (lfc.M_a[a] + M)
-                    Phi[G, c0:c0 + 3 * nm] += ph * A.reshape(len(G), -1)
-                else:
-                    c0 = lfc.M_a[a] + M
-                    Phi[G, c0:c0 + nm] += ph * A
+                c0 = lfc.M_a[a] + M
+                Phi[G, c0:c0 + nm] += ph * A
             M += nm
     return Phi
 
@@ -102,8 +97,15 @@ def test_merged_volumes_match_per_function_boxes(name, monkeypatch):
     got = dense(lfc.lfc, q)
     want = dense_reference(gd, lfc, spos, q)
     assert np.abs(got - want).max() == 0.0
-    if k is None:
-        d = lfc._derivative_object()
-        got = dense(d)
-        want = dense_reference(gd, lfc, spos, derivative=True)
-        assert np.abs(got - want).max() < 1e-14 * np.abs(want).max()
+    # the derivative's arguments: one spline per M in M order, and each
+    # merged volume centred on its atom's periodic image
+    spline_M, pos_Wv = lfc._derivative_arguments()
+    assert len(spline_M) == lfc.Mmax
+    for a, sphere in enumerate(lfc.sphere_a):
+        M = lfc.M_a[a]
+        for spline in sphere.spline_j:
+            for m in range(2 * spline.l + 1):
+                assert spline_M[M + m] is spline
+            M += 2 * spline.l + 1
+    for W, ((a, _, _), sd) in enumerate(zip(lfc.box_W, lfc.sdisp_Wc)):
+        assert np.allclose(pos_Wv[W], (spos[a] - sd) @ gd.cell_cv)

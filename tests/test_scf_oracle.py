@@ -27,14 +27,6 @@ pytestmark = pytest.mark.skipif(not ref.available(),
 TIGHT = dict(energy_tol=1e-7, density_tol=1e-6, eigenstates_tol=1e-11)
 
 
-def setup_data(s):
-    """A gpaw_b200.hgh.HGHSetup as the oracle's plain radial data."""
-    sp = lambda x: (x.l, x.rmax, np.array(x.f_g))
-    return dict(Z=s.Z, rloc=s.rloc, r_gauss=s.r_gauss, vbar=sp(s.vbar),
-                ghat=sp(s.ghat), nguess=sp(s.nguess),
-                pt=[sp(p) for p in s.pt_j], dH=np.asarray(s.dH_ii, float))
-
-
 def system(name):
     from gpaw_b200.scf import h2, si_diamond
     if name == 'H2':
@@ -55,7 +47,7 @@ def cpu_start(name, seed=0):
     pbc_c = np.array([pbc] * 3)
     N_c = osf.h2gpts(h / bohr, cell_cv)
     kinds = {s: HGHSetup(s) for s in set(sym)}
-    setups = [setup_data(kinds[s]) for s in sym]
+    setups = [osf.setup_data(kinds[s]) for s in sym]
     spos = np.linalg.solve(cell_cv.T, (np.asarray(pos) / bohr).T).T
     if pbc:
         spos %= 1.0
@@ -112,10 +104,7 @@ def oracle_for(calc):
     """The oracle on the device calculation's geometry, setups and start
     (its orthonormalised initial wave functions, widened to FP64)."""
     from oracle import scf as osf
-    kpt = calc.wfs.kpt_u[0]
-    return osf.SCF([setup_data(s) for s in calc.setups], calc.spos_ac, calc.cell_cv,
-                   calc.pbc, calc.gd.N_c, kpt.psit_nG.double().cpu().numpy(),
-                   np.asarray(kpt.f_n), xc='LDA', mixer_beta=calc.mixer.beta)
+    return osf.from_calculation(calc, xc='LDA')
 
 
 def rel(a, b):
