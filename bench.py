@@ -410,6 +410,38 @@ def scf_cpu_baseline(make_calc, iterations, sample_iterations=1):
                       f'{iterations} iterations of the plain FP64 form'}
 
 
+def precision_benchmark():
+    """The precision configuration: 32 H2O molecules (O-H 0.96 A, 104.5 deg,
+    seeded orientations, 4 x 4 x 2 lattice of 3.1 A plus 0.1 A jitter) in a
+    15 A box with zero boundaries, h = 0.2 A (76^3), 160 bands (128
+    occupied), PBE, Pulay mixing 0.1.  The FP64 run and the FP32 run from
+    the same start; the FP32 errors in total energy (eV per valence
+    electron), occupied eigenvalues (eV) and forces (eV / A) against FP64."""
+    import torch
+    from gpaw_b200.scf import Calculation, h2o_cluster
+    sym, pos, cell = h2o_cluster()
+    runs = {}
+    for prec, tol in (('fp64', 1e-7), ('fp32', 1e-6)):
+        c = Calculation(sym, pos, cell, False, h=0.2, nbands=160, xc='PBE',
+                        precision=prec, mixer_beta=0.1)
+        log = c.run(maxiter=300, energy_tol=tol, graph=True)
+        runs[prec] = dict(converged=log.converged, iterations=log.iterations,
+                          seconds=round(log.wall, 3), energy_eV=log.energies[-1],
+                          eps=c.eigenvalues()[:128], F=c.forces(), nel=c.nvalence)
+        del c
+        gc.collect()
+        torch.cuda.empty_cache()
+    a, b = runs['fp64'], runs['fp32']
+    return {'workload': '(H2O)32, 15 A box, zero boundaries, h=0.2 A (76^3), 160 bands, '
+                        'PBE, FP32 vs FP64 from the same start',
+            'fp64': {k: a[k] for k in ('converged', 'iterations', 'seconds', 'energy_eV')},
+            'fp32': {k: b[k] for k in ('converged', 'iterations', 'seconds', 'energy_eV')},
+            'energy_error_eV_per_electron': float(abs(a['energy_eV'] - b['energy_eV']) / a['nel']),
+            'max_occupied_eigenvalue_error_eV': float(np.abs(a['eps'] - b['eps']).max()),
+            'max_force_error_eV_per_A': float(np.abs(a['F'] - b['F']).max()),
+            'max_force_eV_per_A': float(np.abs(a['F']).max())}
+
+
 def lfc_benchmark(args):
     """The projector LFC of the Si64 SCF on its production shape: 64 Si
     atoms (2 s + 2 p radial functions merged into 8 functions per atom), the
@@ -749,8 +781,10 @@ def main():
     e2e_value = world * nbytes / (e2e_ms / 1e3) / 1e9
 
     scf_res = None
+    prec_res = None
     if not args.no_scf and rank == 0:
         scf_res = scf_benchmark()
+        prec_res = precision_benchmark()
     suite_res = None
     if not args.no_suite:
         del x, y
@@ -796,6 +830,7 @@ def main():
         'cpu_baseline': cpu,
         'suite_GBps': suite_res,
         'scf': scf_res,
+        'precision': prec_res,
     }
     if rank == 0:
         print(json.dumps(line))

@@ -464,6 +464,88 @@ class Calculation:
         eps = eps.cpu().numpy() if isinstance(eps, torch.Tensor) else np.asarray(eps)
         return eps * Hartree
 
+    # -------------------------------------------------------------- forces
+    def forces(self):
+        """Hellmann-Feynman forces (eV / Angstrom, natoms x 3) of the
+        converged state: minus the derivative of the total energy with
+        respect to each atom's position at fixed wave functions and density
+        (the terms gpaw/forces.py collects from the wave functions, the
+        local potential and the compensation charges,
+        gpaw/wavefunctions/fdpw.py:426-450, gpaw/hamiltonian.py:408, 803):
+          projectors     2 sum_n f_n sum_ij <psi_n|d p^a_i/dr> dH^a_ij P^a_nj
+          vbar           int nt d vbar^a/dr
+          ion charges    -(derivative of int v_H rhot through the Gaussian
+                         ion charge -Z g/I(R), normalised on the grid)
+          ion-ion        the geometry constant's gradient
+        Device work in the precision of the run (sums in FP64); the small
+        per-atom reductions on the host."""
+        kpt = self.wfs.kpt_u[0]
+        natoms = len(self.setups)
+        F = np.zeros((natoms, 3))
+        pt = self.wfs.pt
+        f_n = torch.as_tensor(np.asarray(kpt.f_n, float), device=self.gd.device)
+        if pt.Mmax:
+            D = pt.derivative(kpt.psit_nG, {}, kpt.q if self.dtype.is_complex else -1)
+            P = kpt.P_nM.to(torch.float64)
+            C = P @ self.dH_MM.T
+            F_Mv = 2 * (f_n[:, None, None] * D.to(torch.float64) * C[:, :, None]).sum(0)
+            F_Mv = F_Mv.cpu().numpy()
+            for a in range(natoms):
+                M = pt.M_a[a]
+                F[a] += F_Mv[M:M + self.setups[a].ni].sum(0)
+        # local potential: d/dR int nt vbar = -int nt dvbar/dr
+        Dv = self.vbar.derivative(self.nt_g, {}).cpu().numpy()      # (natoms, 3)
+        F += Dv
+        # ion charges rho_a = -Z g(r - R) / I(R), I = dv sum_g g:
+        # dE/dR = Z [D(v_H) / I - A(v_H) D(1) / I^2] with D(a) = dv sum a dg/dr,
+        # A(a) = dv sum a g
+        raw = self._ghat_raw()
+        one = torch.ones_like(self.vHt_g)
+        D_v = raw.derivative(self.vHt_g, {}).cpu().numpy()
+        D_1 = raw.derivative(one, {}).cpu().numpy()
+        A_v = raw.integrate(self.vHt_g, {}).cpu().numpy()
+        I = raw.integrate(one, {}).cpu().numpy()
+        Z = np.array([s.Z for s in self.setups], float)
+        F -= Z[:, None] * (D_v / I[:, None] - A_v[:, None] * D_1 / I[:, None]**2)
+        F -= self._constant_energy_gradient()
+        return F * Hartree / Bohr
+
+    def _ghat_raw(self):
+        """The ion-charge functions without their grid normalisation."""
+        if getattr(self, '_ghat_unnormalised', None) is None:
+            g = LFC(self.finegd, [[s.ghat] for s in self.setups], cut=True)
+            g.set_positions(self.spos_ac)
+            self._ghat_unnormalised = g
+        return self._ghat_unnormalised
+
+    def _constant_energy_gradient(self):
+        """d E_0 / d R_a (Hartree / Bohr) of `_constant_energy`."""
+        from scipy.special import erf
+        setups = self.setups
+        Z = np.array([s.Z for s in setups], float)
+        rl = np.array([s.rloc for s in setups])
+        sg = np.array([s.r_gauss for s in setups])
+        pos_av = self.spos_ac @ self.cell_cv
+        w1 = np.sqrt(2 * (rl[:, None]**2 + rl[None, :]**2))
+        w2 = np.sqrt(2 * (sg[:, None]**2 + sg[None, :]**2))
+        ZZ = Z[:, None] * Z[None, :]
+        G = np.zeros((len(setups), 3))
+        shifts = [(-1, 0, 1) if p else (0,) for p in self.pbc]
+
+        def phi_prime(R, w):
+            # d/dR [erf(R / w) / R]
+            return (2 / np.sqrt(np.pi) * np.exp(-(R / w)**2) / (w * R) -
+                    erf(R / w) / R**2)
+        for n_c in itertools.product(*shifts):
+            d = pos_av[None, :, :] + np.dot(n_c, self.cell_cv) - pos_av[:, None, :]
+            R = np.linalg.norm(d, axis=2)
+            if not any(n_c):
+                np.fill_diagonal(R, np.inf)
+            dphi = ZZ * (phi_prime(R, w1) - phi_prime(R, w2))
+            # E_0 = 1/2 sum_ab phi(|R_b + n - R_a|): d/dR_a picks both ends
+            G -= (dphi[:, :, None] * d / R[:, :, None]).sum(1)
+        return G
+
 
 def si_diamond(ncell=1, a=5.43, rattle=0.0, seed=0):
     """Diamond Si, ncell^3 conventional cells (8 atoms each)."""
@@ -480,6 +562,36 @@ def si_diamond(ncell=1, a=5.43, rattle=0.0, seed=0):
         pos += np.random.default_rng(seed).normal(0.0, rattle, pos.shape)
     L = ncell * a
     return ['Si'] * len(pos), pos, [L, L, L]
+
+
+def h2o_cluster(nx=4, ny=4, nz=2, spacing=3.1, box=15.0, jitter=0.1, seed=0,
+                d_oh=0.96, angle=104.5):
+    """(H2O)_{nx ny nz} cluster: water molecules (O-H d_oh, H-O-H angle) with
+    seeded uniformly random orientations (a random rotation from the QR
+    decomposition of a Gaussian matrix, sign-fixed), centred on an
+    nx x ny x nz lattice of the given spacing plus seeded Gaussian jitter,
+    the lattice centred in a cubic box of side `box` (Angstrom).  The
+    32-molecule precision configuration is the default."""
+    rng = np.random.default_rng(seed)
+    t = np.radians(angle) / 2
+    mol = np.array([[0.0, 0.0, 0.0],
+                    [d_oh * np.sin(t), 0.0, d_oh * np.cos(t)],
+                    [-d_oh * np.sin(t), 0.0, d_oh * np.cos(t)]])
+    mol -= mol.mean(0)
+    sym, pos = [], []
+    lat = np.array([(i, j, k) for i in range(nx) for j in range(ny) for k in range(nz)],
+                   float) * spacing
+    lat += box / 2 - lat.mean(0)
+    for c in lat:
+        q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+        q = q * np.sign(np.diag(r))
+        if np.linalg.det(q) < 0:
+            q[:, 0] = -q[:, 0]
+        centre = c + rng.normal(0.0, jitter, 3)
+        for s, p in zip(('O', 'H', 'H'), mol @ q.T + centre):
+            sym.append(s)
+            pos.append(p)
+    return sym, np.array(pos), [box, box, box]
 
 
 def h2(vacuum=3.0, d=0.74):

@@ -110,6 +110,8 @@ class LFC:
         self.M_a = []
         M = 0
         W = 0
+        self.spline_M = []      # _gpaw.Spline per M (LFC.derivative's argument)
+        pos_W = []
         for a, spl in enumerate(splines_a):
             self.M_a.append(M)
             A_w, Mw_w = [], []
@@ -118,6 +120,7 @@ class LFC:
                 f = np.array(f_g, float)
                 f[-1] = 0.0
                 s = gp.Spline(int(l), float(rmax), f)
+                self.spline_M.extend([s] * (2 * int(l) + 1))
                 for beg, end, sdisp in boxes(g, spos_ac[a], rmax):
                     pos_v = (np.asarray(spos_ac[a]) - sdisp) @ g.cell_cv
                     A_gm, G_b = gp.spline_to_grid(s, beg, end, pos_v,
@@ -128,6 +131,7 @@ class LFC:
                     A_w.append(A_gm)
                     Mw_w.append(Ml)
                     G_l.append(G_b)
+                    pos_W.append(pos_v)
                     w = np.empty(len(G_b), np.intc)
                     w[0::2] = W
                     w[1::2] = -W - 1
@@ -149,6 +153,7 @@ class LFC:
             M_W.extend(M + m for m in Mw_w)
             M += Ml
         self.Mmax = M
+        self.pos_Wv = np.ascontiguousarray(np.array(pos_W).reshape(-1, 3), float)
         if not A_W:                 # no functions (e.g. H has no projectors)
             self.lfc = None
             return
@@ -171,6 +176,17 @@ class LFC:
         c = np.zeros(a_xG.shape[:-3] + (self.Mmax,))
         if self.lfc is not None:
             self.lfc.integrate(np.ascontiguousarray(a_xG), c, -1)
+        return c
+
+    def derivative(self, a_xG):
+        """dv sum_G a_xG dPhi_M/dr_v: the reference's LFC.derivative with
+        the arguments gpaw/lfc.py:660-682 builds."""
+        c = np.zeros(a_xG.shape[:-3] + (self.Mmax, 3))
+        if self.lfc is not None:
+            g = self.g
+            self.lfc.derivative(np.ascontiguousarray(a_xG), c,
+                                np.ascontiguousarray(g.h_cv), g.n_c, self.spline_M,
+                                g.beg_c, self.pos_Wv, -1)
         return c
 
 
@@ -330,8 +346,10 @@ class SCF:
             M = self.pt.M_a[a]
             self.dH_MM[M:M + ni, M:M + ni] = s['dH']
         vbar = LFC(fine, [[s['vbar']] for s in setups], self.spos_ac)
+        self.vbar = vbar
         self.vbar_g = np.zeros(tuple(fine.n_c))
         vbar.add(self.vbar_g, np.ones((len(setups),)))
+        self.ghat_raw = LFC(fine, [[s['ghat']] for s in setups], self.spos_ac)
         ghat = LFC(fine, [[s['ghat']] for s in setups], self.spos_ac,
                    integral=[float(s['Z']) for s in setups])
         self.rhoion_g = np.zeros(tuple(fine.n_c))
@@ -404,6 +422,7 @@ class SCF:
             gp.XCFunctional(0).calculate(e_g, n_sg, v_sg, sigma, dedsigma)
             for v in range(3):
                 v_sg[0] -= 2.0 * self.grads[v](dedsigma[0] * grad_vg[v])
+        self.vHt_g = vHt_g
         self.vt_g = self.vbar_g + vHt_g + v_sg[0]
         self.vt_G = self.restrict(self.vt_g)
         self.e_terms = np.array([0.5 * (rhot_g * vHt_g).sum() * fine.dv,
@@ -545,3 +564,42 @@ class SCF:
 
     def eigenvalues(self):
         return self.eps * HARTREE
+
+    # ---------------------------------------------------------- forces
+    def forces(self):
+        """Hellmann-Feynman forces (eV / Angstrom) of the present state:
+        projectors 2 sum_n f_n sum_ij <psi|dp_i/dr> dH_ij P_nj (the
+        reference's LFC.derivative on the wave functions), vbar
+        int nt dvbar/dr, the grid-normalised Gaussian ion charges
+        -Z [D(v_H) / I - A(v_H) D(1) / I^2] and the gradient of the
+        geometry constant, by central differences of its closed form."""
+        natoms = len(self.setups)
+        F = np.zeros((natoms, 3))
+        if self.pt.Mmax:
+            D = self.pt.derivative(self.psit)                  # (nb, M, 3)
+            C = self.P @ self.dH_MM.T
+            F_Mv = 2 * np.einsum('n,nmv,nm->mv', self.f_n, D, C)
+            for a, s in enumerate(self.setups):
+                M = self.pt.M_a[a]
+                F[a] += F_Mv[M:M + len(s['dH'])].sum(0)
+        F += self.vbar.derivative(self.nt_g)
+        one = np.ones_like(self.vHt_g)
+        D_v = self.ghat_raw.derivative(self.vHt_g)
+        D_1 = self.ghat_raw.derivative(one)
+        A_v = self.ghat_raw.integrate(self.vHt_g)
+        I = self.ghat_raw.integrate(one)
+        Z = np.array([s['Z'] for s in self.setups], float)
+        F -= Z[:, None] * (D_v / I[:, None] - A_v[:, None] * D_1 / I[:, None]**2)
+        h = 1e-5
+        for a in range(natoms):
+            for v in range(3):
+                e = []
+                for sgn in (1, -1):
+                    spos = self.spos_ac.copy()
+                    spos[a] += sgn * h * np.linalg.inv(self.g.cell_cv)[v]
+                    saved = self.spos_ac
+                    self.spos_ac = spos
+                    e.append(self._constant_energy())
+                    self.spos_ac = saved
+                F[a, v] -= (e[0] - e[1]) / (2 * h)
+        return F * HARTREE / 0.52917721067
