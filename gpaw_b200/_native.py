@@ -100,6 +100,15 @@ _SIGNATURES = {
                                   c_void_p, P64, P64, c_void_p]),
     'gb_lfc_derivative': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, PD, P64,
                                   POINTER(c_void_p), P64, PD, c_int, c_int, c_void_p]),
+    'gb_operator_apply_k': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int,
+                                    PD, c_void_p, c_void_p]),
+    'gb_transformer_apply_k': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int,
+                                       PD, c_void_p]),
+    'gb_fd_precond_k': (c_int, [c_void_p] * 7 + [c_void_p] * 8 +
+                        [c_void_p, c_double, c_int64, c_int, c_int, PD, c_void_p]),
+    'gb_lfc_add_k': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
+    'gb_lfc_integrate_k': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int,
+                                   c_void_p]),
     'gb_xc_calculate': (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_void_p, c_void_p]),
     'gb_fd_precond': (c_int, [c_void_p] * 7 + [c_void_p] * 8 +
@@ -149,6 +158,21 @@ def phases(phase_cd) -> ctypes.Array | None:
         phase_cd = phase_cd.detach().cpu().numpy()
     p = np.asarray(phase_cd, dtype=complex).reshape(3, 2)
     return f64(np.stack([p.real, p.imag], axis=-1))
+
+
+def phase_sets(phase_cd):
+    """(nk, 3, 2) complex Bloch phases (one set per k-point of a batch) ->
+    (nk, ctypes array of nk x 12 doubles), or (1, 12 doubles) for a single
+    (3, 2) set."""
+    if isinstance(phase_cd, torch.Tensor):
+        phase_cd = phase_cd.detach().cpu().numpy()
+    p = np.asarray(phase_cd, dtype=complex).reshape(-1, 3, 2)
+    return len(p), f64(np.stack([p.real, p.imag], axis=-1))
+
+
+def is_phase_batch(phase_cd) -> bool:
+    """True for (nk, 3, 2) phases with nk > 1 (a k-point batch)."""
+    return phase_cd is not None and np.ndim(phase_cd) == 3 and np.shape(phase_cd)[0] > 1
 
 
 def dtype_code(t: torch.Tensor) -> int:

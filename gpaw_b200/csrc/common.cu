@@ -1,6 +1,6 @@
 // Error state, device queries and version for libgpawb200.
 #include <string>
-#include "common.cuh"
+#include "internal.cuh"
 
 namespace gb {
 
@@ -30,6 +30,21 @@ int sm_count() {
     cached[dev] = n > 0 ? n : 1;
   }
   return cached[dev];
+}
+
+void fill_phase_sets(PhaseSets& p, const double* src, int nk, int64_t nbatch) {
+  p.nk = nk < 1 ? 1 : nk;
+  p.per_k = p.nk > 1 ? nbatch / p.nk : nbatch;
+  if (p.per_k < 1) p.per_k = 1;
+  p.any = 0;
+  for (int k = 0; k < KMAX; ++k)
+    for (int c = 0; c < 3; ++c)
+      for (int d = 0; d < 2; ++d) {
+        const bool have = src && k < p.nk;
+        p.ph[k][c][d][0] = have ? src[k * 12 + (c * 2 + d) * 2] : 1.0;
+        p.ph[k][c][d][1] = have ? src[k * 12 + (c * 2 + d) * 2 + 1] : 0.0;
+        if (p.ph[k][c][d][0] != 1.0 || p.ph[k][c][d][1] != 0.0) p.any = 1;
+      }
 }
 
 }  // namespace gb

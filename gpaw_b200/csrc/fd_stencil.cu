@@ -38,11 +38,10 @@ struct StarArgs {
   int n0, n1, n2;
   int pbc0, pbc1, pbc2;
   int tiles1, tiles2;
-  int has_phase;
   double c0;
   double c0diff;              // c0 + sum of the neighbour coefficients (difference form)
   double a[3][2 * HMAX + 1];  // a[axis][m + HMAX]: coefficient of offset m (m != 0)
-  double ph[3][2][2];         // ph[axis][side][re/im]
+  PhaseSets phs;              // Bloch phases per k-point group of bands
   // epilogue: out = alpha * S(in) + beta * in + gamma * y   (y may be null)
   double alpha, beta, gamma;
   const void* y;
@@ -124,6 +123,7 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
     const T* __restrict__ src = reinterpret_cast<const T*>(args.in) + band * n012;
     T* __restrict__ dst = reinterpret_cast<T*>(args.out) + band * n012;
     const T* __restrict__ ybase = args.y ? reinterpret_cast<const T*>(args.y) + band * n012 : nullptr;
+    const auto& PH = args.phs.ph[phase_set_of(args.phs, band)];
     const bool edge = (y0 - H < 0) || (y0 + T1 + H > n1) || (z0 - HZ < 0) || (z0 + T2 + HZ > n2);
 
     const int j0 = p_start - H, j1 = p_end + H;   // planes pushed: [j0, j1)
@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
       if (j >= 0 && j < n0) return j;
       if (!args.pbc0) return -1;
       const int side = j < 0 ? 1 : 0;
-      pr = args.ph[0][side][0]; pi = args.ph[0][side][1];
+      pr = PH[0][side][0]; pi = PH[0][side][1];
       return wrap_index(j, n0);
     };
 
@@ -200,10 +200,10 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
         const int y = y0 - H + Rw, z = z0 - HZ + k * VEC + v;
         double pr = 1.0, pi = 0.0;
         bool w = false;
-        if (args.pbc1 && (y < 0 || y >= n1)) { const int sd = y < 0; pr = args.ph[1][sd][0]; pi = args.ph[1][sd][1]; w = true; }
+        if (args.pbc1 && (y < 0 || y >= n1)) { const int sd = y < 0; pr = PH[1][sd][0]; pi = PH[1][sd][1]; w = true; }
         if (args.pbc2 && (z < 0 || z >= n2)) {
           const int sd = z < 0;
-          const double qr = args.ph[2][sd][0], qi = args.ph[2][sd][1];
+          const double qr = PH[2][sd][0], qi = PH[2][sd][1];
           const double tr = pr * qr - pi * qi, ti = pr * qi + pi * qr;
           pr = tr; pi = ti; w = true;
         }
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(C::NT, 2) star_kernel(const StarArgs args) {
       double pr, pi;
       const int sp = plane_src(j, pr, pi);
       T* P = planes + ((j - j0) % NS) * PLANE;
-      if (CPLX && args.has_phase && edge && sp >= 0) {
+      if (CPLX && args.phs.any && edge && sp >= 0) {
         fixup(P);
         __syncthreads();
       }
@@ -365,12 +365,11 @@ struct BoxArgs {
   int pbc0, pbc1, pbc2;
   int M;                  // halo radius
   int np;
-  int has_phase;
   int b0, b1, b2;         // tile extents
   int tiles0, tiles1, tiles2;
   double coef[64];
   int off[64][3];
-  double ph[3][2][2];
+  PhaseSets phs;
   double alpha, beta, gamma;
   const void* y;
   const void* vpot;
@@ -395,6 +394,7 @@ __global__ void __launch_bounds__(256) box_kernel(const BoxArgs args) {
     const int z0 = (t % args.tiles2) * args.b2;
     const T* src = reinterpret_cast<const T*>(args.in) + band * n012;
     T* dst = reinterpret_cast<T*>(args.out) + band * n012;
+    const auto& PH = args.phs.ph[phase_set_of(args.phs, band)];
     __syncthreads();
     for (int e = threadIdx.x; e < E0 * E1 * E2; e += blockDim.x) {
       const int i2 = e % E2, i1 = (e / E2) % E1, i0 = e / (E1 * E2);
@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(256) box_kernel(const BoxArgs args) {
         if (g[c] < 0 || g[c] >= n[c]) {
           if (!pbc[c]) { zero_cell = true; break; }
           const int sd = g[c] < 0;
-          const double qr = args.ph[c][sd][0], qi = args.ph[c][sd][1];
+          const double qr = PH[c][sd][0], qi = PH[c][sd][1];
           const double tr = pr * qr - pi * qi, ti = pr * qi + pi * qr;
           pr = tr; pi = ti;
           g[c] = wrap_index(g[c], n[c]);
@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(256) box_kernel(const BoxArgs args) {
       T v = zero<T>();
       if (!zero_cell) {
         v = src[(int64_t)g[0] * n12 + (int64_t)g[1] * args.n2 + g[2]];
-        if (args.has_phase) v = phase_mul(v, pr, pi);
+        if (args.phs.any) v = phase_mul(v, pr, pi);
       }
       tile[e] = v;
     }
@@ -479,7 +479,7 @@ namespace gb {
 
 template <class C>
 static int launch_star(const gb_operator* op, const void* in, void* out, int64_t nin,
-                       const double* phase_cd, cudaStream_t stream, const Epilogue& ep) {
+                       const double* phase_cd, cudaStream_t stream, const Epilogue& ep, int nk) {
   static int occ = -1;
   static size_t smem_set = 0;
   if (smem_set != C::SMEM) {
@@ -502,13 +502,7 @@ static int launch_star(const gb_operator* op, const void* in, void* out, int64_t
     for (int m = 0; m < 2 * HMAX + 1; ++m) a.c0diff += op->a[c][m];
   memcpy(a.a, op->a, sizeof(a.a));
   a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma; a.y = ep.y; a.vpot = ep.vpot;
-  a.has_phase = 0;
-  for (int c = 0; c < 3; ++c)
-    for (int d = 0; d < 2; ++d) {
-      a.ph[c][d][0] = phase_cd ? phase_cd[(c * 2 + d) * 2] : 1.0;
-      a.ph[c][d][1] = phase_cd ? phase_cd[(c * 2 + d) * 2 + 1] : 0.0;
-      if (a.ph[c][d][0] != 1.0 || a.ph[c][d][1] != 0.0) a.has_phase = 1;
-    }
+  fill_phase_sets(a.phs, phase_cd, nk, nin);
   const int64_t total = nin * (int64_t)a.tiles1 * a.tiles2 * a.n0;
   int64_t blocks = (int64_t)sm_count() * occ;
   // keep at least a few planes per CTA so the prologue (2H planes) stays small
@@ -613,7 +607,7 @@ template <int H> struct StarTile<double2, H> { using C = StarCfg<double2, H, (H 
 
 template <typename T>
 static int dispatch_star(const gb_operator* op, const void* in, void* out, int64_t nin,
-                         const double* ph, cudaStream_t st, const Epilogue& ep) {
+                         const double* ph, cudaStream_t st, const Epilogue& ep, int nk) {
   if constexpr (!Elem<T>::cplx) {
     // tiles of star_kernel less than a quarter used: one thread per point
     using C1 = typename StarTile<T, 1>::C;
@@ -628,17 +622,18 @@ static int dispatch_star(const gb_operator* op, const void* in, void* out, int64
     }
   }
   switch (op->H) {
-    case 1: return launch_star<typename StarTile<T, 1>::C>(op, in, out, nin, ph, st, ep);
-    case 2: return launch_star<typename StarTile<T, 2>::C>(op, in, out, nin, ph, st, ep);
-    case 3: return launch_star<typename StarTile<T, 3>::C>(op, in, out, nin, ph, st, ep);
-    case 4: return launch_star<typename StarTile<T, 4>::C>(op, in, out, nin, ph, st, ep);
+    case 1: return launch_star<typename StarTile<T, 1>::C>(op, in, out, nin, ph, st, ep, nk);
+    case 2: return launch_star<typename StarTile<T, 2>::C>(op, in, out, nin, ph, st, ep, nk);
+    case 3: return launch_star<typename StarTile<T, 3>::C>(op, in, out, nin, ph, st, ep, nk);
+    case 4: return launch_star<typename StarTile<T, 4>::C>(op, in, out, nin, ph, st, ep, nk);
     case 5:
-    case 6: return launch_star<typename StarTile<T, 6>::C>(op, in, out, nin, ph, st, ep);
+    case 6: return launch_star<typename StarTile<T, 6>::C>(op, in, out, nin, ph, st, ep, nk);
     default: return fail(GB_E_UNSUPPORTED, "star stencil radius > 6");
   }
 }
 
-static void fill_box_args(const gb_operator* op, BoxArgs& a, const double* phase_cd) {
+static void fill_box_args(const gb_operator* op, BoxArgs& a, const double* phase_cd, int nk = 1,
+                          int64_t nbatch = 1) {
   memset(&a, 0, sizeof(a));
   a.alpha = 1.0;
   a.n0 = (int)op->n[0]; a.n1 = (int)op->n[1]; a.n2 = (int)op->n[2];
@@ -651,19 +646,14 @@ static void fill_box_args(const gb_operator* op, BoxArgs& a, const double* phase
     a.csum += op->coef[p];
     for (int c = 0; c < 3; ++c) a.off[p][c] = op->off[p * 3 + c];
   }
-  for (int c = 0; c < 3; ++c)
-    for (int d = 0; d < 2; ++d) {
-      a.ph[c][d][0] = phase_cd ? phase_cd[(c * 2 + d) * 2] : 1.0;
-      a.ph[c][d][1] = phase_cd ? phase_cd[(c * 2 + d) * 2 + 1] : 0.0;
-      if (a.ph[c][d][0] != 1.0 || a.ph[c][d][1] != 0.0) a.has_phase = 1;
-    }
+  fill_phase_sets(a.phs, phase_cd, nk, nbatch);
 }
 
 template <typename T>
 static int launch_box(const gb_operator* op, const void* in, void* out, int64_t nin,
-                      const double* phase_cd, cudaStream_t stream, const Epilogue& ep) {
+                      const double* phase_cd, cudaStream_t stream, const Epilogue& ep, int nk) {
   BoxArgs a;
-  fill_box_args(op, a, phase_cd);
+  fill_box_args(op, a, phase_cd, nk, nin);
   a.alpha = ep.alpha; a.beta = ep.beta; a.gamma = ep.gamma; a.y = ep.y;
   a.in = in; a.out = out; a.nbatch = nin;
   a.b0 = 4; a.b1 = 8; a.b2 = 32;
@@ -683,24 +673,26 @@ static int launch_box(const gb_operator* op, const void* in, void* out, int64_t 
 
 // internal entry used by gb_operator_apply and the preconditioner chain
 int op_apply(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype,
-             const double* ph, cudaStream_t st, const Epilogue& ep) {
+             const double* ph, cudaStream_t st, const Epilogue& ep, int nk) {
+  if (nk > KMAX) return fail(GB_E_UNSUPPORTED, "more k-point phase sets than one launch takes");
+  if (nk > 1 && nin % nk) return fail(GB_E_INVALID, "batch not divisible by the number of phase sets");
   if (op->cfd) {
-    const int rc = star_tma_apply(op, in, out, nin, dtype, ph, st, ep);
+    const int rc = star_tma_apply(op, in, out, nin, dtype, ph, st, ep, nk);
     if (rc != 1) return rc;
     if (stencil_path() == 2)
       return fail(GB_E_UNSUPPORTED, std::string("TMA stencil path required but not applicable: ") + tma_reason());
     switch (dtype) {
-      case GB_DTYPE_F64: return dispatch_star<double>(op, in, out, nin, ph, st, ep);
-      case GB_DTYPE_F32: return dispatch_star<float>(op, in, out, nin, ph, st, ep);
-      case GB_DTYPE_C128: return dispatch_star<double2>(op, in, out, nin, ph, st, ep);
-      default: return dispatch_star<float2>(op, in, out, nin, ph, st, ep);
+      case GB_DTYPE_F64: return dispatch_star<double>(op, in, out, nin, ph, st, ep, nk);
+      case GB_DTYPE_F32: return dispatch_star<float>(op, in, out, nin, ph, st, ep, nk);
+      case GB_DTYPE_C128: return dispatch_star<double2>(op, in, out, nin, ph, st, ep, nk);
+      default: return dispatch_star<float2>(op, in, out, nin, ph, st, ep, nk);
     }
   }
   switch (dtype) {
-    case GB_DTYPE_F64: return launch_box<double>(op, in, out, nin, ph, st, ep);
-    case GB_DTYPE_F32: return launch_box<float>(op, in, out, nin, ph, st, ep);
-    case GB_DTYPE_C128: return launch_box<double2>(op, in, out, nin, ph, st, ep);
-    default: return launch_box<float2>(op, in, out, nin, ph, st, ep);
+    case GB_DTYPE_F64: return launch_box<double>(op, in, out, nin, ph, st, ep, nk);
+    case GB_DTYPE_F32: return launch_box<float>(op, in, out, nin, ph, st, ep, nk);
+    case GB_DTYPE_C128: return launch_box<double2>(op, in, out, nin, ph, st, ep, nk);
+    default: return launch_box<float2>(op, in, out, nin, ph, st, ep, nk);
   }
 }
 
@@ -801,6 +793,23 @@ int gb_operator_apply_potential(const gb_operator* op, const void* in, void* out
   Epilogue ep;
   ep.vpot = vt;
   return op_apply(op, in, out, nin, dtype, dtype_complex(dtype) ? phase_cd : nullptr, (cudaStream_t)stream, ep);
+}
+
+int gb_operator_apply_k(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype, int nk,
+                        const double* phase_kcd, const void* vt, void* stream) {
+  GB_REQUIRE(op, "gb_operator_apply_k: null operator");
+  GB_REQUIRE(dtype_valid(dtype) && nin >= 0, "gb_operator_apply_k: bad dtype or batch");
+  GB_REQUIRE(dtype_complex(dtype) == !op->real,
+             "gb_operator_apply_k: dtype does not match the operator's real/complex flag");
+  GB_REQUIRE(nk >= 1 && nk <= KMAX, "gb_operator_apply_k: nk must be 1 .. 8");
+  GB_REQUIRE(nin % nk == 0, "gb_operator_apply_k: the batch must split into nk equal groups");
+  if (nin == 0) return GB_OK;
+  GB_REQUIRE(in && out && in != out, "gb_operator_apply_k: bad data pointers");
+  GB_REQUIRE(!dtype_complex(dtype) || phase_kcd, "gb_operator_apply_k: complex data needs phases");
+  Epilogue ep;
+  ep.vpot = vt;
+  return op_apply(op, in, out, nin, dtype, dtype_complex(dtype) ? phase_kcd : nullptr, (cudaStream_t)stream, ep,
+                  nk);
 }
 
 int gb_operator_relax(const gb_operator* op, int relax_method, double* f_g, const double* s_g,

@@ -644,12 +644,12 @@ static int g_stencil_path = 0;   // 0 auto, 1 cp.async only, 2 TMA required
 const char* tma_reason() { return g_tma_reason; }
 
 int star_tma_apply(const gb_operator* op, const void* in, void* out, int64_t nin, int dtype, const double* ph,
-                   cudaStream_t st, const Epilogue& ep) {
+                   cudaStream_t st, const Epilogue& ep, int nk) {
   g_tma_reason = "";
   if (g_stencil_path == 1) { g_tma_reason = "cp.async path forced"; return 1; }
   if (!op->cfd || op->H > 4) { g_tma_reason = "stencil not on axes or radius > 4"; return 1; }
   if (ph) {
-    for (int i = 0; i < 6; ++i)
+    for (int i = 0; i < 6 * (nk > 1 ? nk : 1); ++i)
       if (ph[2 * i] != 1.0 || ph[2 * i + 1] != 0.0) { g_tma_reason = "Bloch phases"; return 1; }
   }
   const size_t es = dtype_size(dtype);

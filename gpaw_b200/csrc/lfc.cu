@@ -166,7 +166,7 @@ __device__ __forceinline__ void load_row(const V* __restrict__ src, int nm, V (&
 template <typename T, int XB, int NMAX>
 __global__ void __launch_bounds__(256) lfc_add_kernel(const LfcView l, const typename AType<T>::A* __restrict__ A,
                                                       const T* __restrict__ c_xM, T* __restrict__ a_xG, int64_t nx,
-                                                      int q) {
+                                                      int q, int64_t per_q) {
   using R = typename Elem<T>::R;
   constexpr bool CPLX = Elem<T>::cplx;
   const int64_t x0 = (int64_t)blockIdx.y * XB;
@@ -186,13 +186,18 @@ __global__ void __launch_bounds__(256) lfc_add_kernel(const LfcView l, const typ
 #pragma unroll
       for (int m = 0; m < NMAX; ++m) Av[m] = (R)Aw[m];
       double pr = 1.0, pi = 0.0;
-      if (CPLX && q >= 0) {
+      if (CPLX && q >= 0 && per_q == 0) {
         const double2 ph = l.phase[(int64_t)q * l.nW + l.ct_W[c]];
         pr = ph.x; pi = -ph.y;   // conj(phase) (c/lfc.c:864)
       }
 #pragma unroll
       for (int i = 0; i < XB; ++i) {
         if (i < nb) {
+          if (CPLX && q >= 0 && per_q > 0) {
+            // k-point of this band: q + band / per_q
+            const double2 ph = l.phase[(q + (x0 + i) / per_q) * l.nW + l.ct_W[c]];
+            pr = ph.x; pi = -ph.y;
+          }
           const T* cx = c_xM + (x0 + i) * l.nM + M;
           T s = zero<T>();
           if constexpr (!CPLX) {
@@ -225,7 +230,7 @@ __global__ void __launch_bounds__(256) lfc_add_kernel(const LfcView l, const typ
 template <typename T, int NM, int XB, int NT>
 __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, const typename AType<T>::A* __restrict__ A,
                                                           const T* __restrict__ a_xG, T* __restrict__ c_xM,
-                                                          int64_t nx, int q, int group_base) {
+                                                          int64_t nx, int q, int group_base, int64_t per_q) {
   using R = typename Elem<T>::R;
   constexpr bool CPLX = Elem<T>::cplx;
   __shared__ T red[NT / 32][XB * NM];
@@ -290,9 +295,15 @@ __global__ void __launch_bounds__(NT) lfc_integrate_kernel(const LfcView l, cons
         }
       }
 #pragma unroll
-      for (int i = 0; i < XB; ++i)
+      for (int i = 0; i < XB; ++i) {
+        double qr = pr, qi = pi;
+        if (q >= 0 && per_q > 0 && x0 + i < nx) {
+          const double2 ph = l.phase[(q + (x0 + i) / per_q) * l.nW + W];
+          qr = ph.x; qi = ph.y;
+        }
 #pragma unroll
-        for (int m = 0; m < NM; ++m) acc[i][m] = add(acc[i][m], phase_mul(part[i][m], pr, pi));
+        for (int m = 0; m < NM; ++m) acc[i][m] = add(acc[i][m], phase_mul(part[i][m], qr, qi));
+      }
     }
   }
   // block reduction: warp shuffles, then across warps
@@ -467,6 +478,7 @@ __global__ void __launch_bounds__(256) lfc_add_bands_kernel(const int* __restric
 
 template <typename T, int NM>
 static int integrate_nm(const gb_lfc* l, int gbeg, int gcount, const void* a, void* c, int64_t nx, int q,
+                        int64_t per_q,
                         cudaStream_t st) {
   // accumulators per thread: XB x NM (twice that for complex images)
   constexpr int XB0 = NM <= 2 ? 16 : (NM <= 4 ? 8 : (NM <= 8 ? 4 : (NM <= 16 ? 2 : 1)));
@@ -475,7 +487,7 @@ static int integrate_nm(const gb_lfc* l, int gbeg, int gcount, const void* a, vo
   const typename AType<T>::A* A;
   if constexpr (std::is_same<typename AType<T>::A, float>::value) A = l->A32; else A = l->A64;
   dim3 grid((unsigned)gcount, (unsigned)((nx + XB - 1) / XB));
-  lfc_integrate_kernel<T, NM, XB, NT><<<grid, NT, 0, st>>>(view(l), A, (const T*)a, (T*)c, nx, q, gbeg);
+  lfc_integrate_kernel<T, NM, XB, NT><<<grid, NT, 0, st>>>(view(l), A, (const T*)a, (T*)c, nx, q, gbeg, per_q);
   return check_launch("lfc_integrate_kernel");
 }
 
@@ -509,7 +521,8 @@ static int add_fast(const gb_lfc* l, const void* c, void* a, int64_t nx, cudaStr
 }
 
 template <typename T>
-static int integrate_t(const gb_lfc* l, const void* a, void* c, int64_t nx, int q, cudaStream_t st) {
+static int integrate_t(const gb_lfc* l, const void* a, void* c, int64_t nx, int q, cudaStream_t st,
+                       int64_t per_q = 0) {
   // groups are sorted by nm on the host; one launch per padded class
   int g = 0;
   while (g < l->ngroups) {
@@ -518,13 +531,13 @@ static int integrate_t(const gb_lfc* l, const void* a, void* c, int64_t nx, int 
     while (e < l->ngroups && nm_class(l->h_gr_nm[e]) == cls) ++e;
     int rc;
     switch (cls) {
-      case 1: rc = integrate_nm<T, 1>(l, g, e - g, a, c, nx, q, st); break;
-      case 2: rc = integrate_nm<T, 2>(l, g, e - g, a, c, nx, q, st); break;
-      case 4: rc = integrate_nm<T, 4>(l, g, e - g, a, c, nx, q, st); break;
-      case 8: rc = integrate_nm<T, 8>(l, g, e - g, a, c, nx, q, st); break;
-      case 16: rc = integrate_nm<T, 16>(l, g, e - g, a, c, nx, q, st); break;
-      case 32: rc = integrate_nm<T, 32>(l, g, e - g, a, c, nx, q, st); break;
-      case 64: rc = integrate_nm<T, 64>(l, g, e - g, a, c, nx, q, st); break;
+      case 1: rc = integrate_nm<T, 1>(l, g, e - g, a, c, nx, q, per_q, st); break;
+      case 2: rc = integrate_nm<T, 2>(l, g, e - g, a, c, nx, q, per_q, st); break;
+      case 4: rc = integrate_nm<T, 4>(l, g, e - g, a, c, nx, q, per_q, st); break;
+      case 8: rc = integrate_nm<T, 8>(l, g, e - g, a, c, nx, q, per_q, st); break;
+      case 16: rc = integrate_nm<T, 16>(l, g, e - g, a, c, nx, q, per_q, st); break;
+      case 32: rc = integrate_nm<T, 32>(l, g, e - g, a, c, nx, q, per_q, st); break;
+      case 64: rc = integrate_nm<T, 64>(l, g, e - g, a, c, nx, q, per_q, st); break;
       default: return fail(GB_E_UNSUPPORTED, "lfc: more than 64 functions in one volume");
     }
     if (rc) return rc;
@@ -534,30 +547,31 @@ static int integrate_t(const gb_lfc* l, const void* a, void* c, int64_t nx, int 
 }
 
 template <typename T, int XB, int NMAX>
-static int add_nm(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st) {
+static int add_nm(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st, int64_t per_q) {
   const typename AType<T>::A* A;
   if constexpr (std::is_same<typename AType<T>::A, float>::value) A = l->A32; else A = l->A64;
   const int NT = 256;
   const int64_t bx = std::min<int64_t>((l->P + NT - 1) / NT, (int64_t)sm_count() * 8);
   dim3 grid((unsigned)bx, (unsigned)((nx + XB - 1) / XB));
-  lfc_add_kernel<T, XB, NMAX><<<grid, NT, 0, st>>>(view(l), A, (const T*)c, (T*)a, nx, q);
+  lfc_add_kernel<T, XB, NMAX><<<grid, NT, 0, st>>>(view(l), A, (const T*)c, (T*)a, nx, q, per_q);
   return check_launch("lfc_add_kernel");
 }
 
 template <typename T>
-static int add_t(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st) {
+static int add_t(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st,
+                 int64_t per_q = 0) {
   if (l->P == 0) return GB_OK;
   if constexpr (!Elem<T>::cplx) {
     if (l->fast_nmax) return add_fast<T>(l, c, a, nx, st);
   }
   switch (nm_class(l->maxnm)) {
-    case 1: return add_nm<T, 8, 1>(l, c, a, nx, q, st);
-    case 2: return add_nm<T, 8, 2>(l, c, a, nx, q, st);
-    case 4: return add_nm<T, 8, 4>(l, c, a, nx, q, st);
-    case 8: return add_nm<T, 8, 8>(l, c, a, nx, q, st);
-    case 16: return add_nm<T, 4, 16>(l, c, a, nx, q, st);
-    case 32: return add_nm<T, 2, 32>(l, c, a, nx, q, st);
-    case 64: return add_nm<T, 1, 64>(l, c, a, nx, q, st);
+    case 1: return add_nm<T, 8, 1>(l, c, a, nx, q, st, per_q);
+    case 2: return add_nm<T, 8, 2>(l, c, a, nx, q, st, per_q);
+    case 4: return add_nm<T, 8, 4>(l, c, a, nx, q, st, per_q);
+    case 8: return add_nm<T, 8, 8>(l, c, a, nx, q, st, per_q);
+    case 16: return add_nm<T, 4, 16>(l, c, a, nx, q, st, per_q);
+    case 32: return add_nm<T, 2, 32>(l, c, a, nx, q, st, per_q);
+    case 64: return add_nm<T, 1, 64>(l, c, a, nx, q, st, per_q);
     default: return fail(GB_E_UNSUPPORTED, "lfc: more than 64 functions in one volume");
   }
 }
@@ -881,6 +895,32 @@ int gb_lfc_integrate(const gb_lfc* l, const void* a_xG, void* c_xM, int64_t nx, 
     case GB_DTYPE_C128: return integrate_t<double2>(l, a_xG, c_xM, nx, q, st);
     default: return integrate_t<float2>(l, a_xG, c_xM, nx, q, st);
   }
+}
+
+int gb_lfc_add_k(const gb_lfc* l, const void* c_xM, void* a_xG, int64_t nx, int dtype, int nk, void* stream) {
+  GB_REQUIRE(l && dtype_valid(dtype) && nx >= 0, "gb_lfc_add_k: bad arguments");
+  GB_REQUIRE(dtype_complex(dtype), "gb_lfc_add_k: k-point batches are complex");
+  GB_REQUIRE(nk >= 1 && nk <= l->nq && nx % nk == 0, "gb_lfc_add_k: nk must divide the batch and be <= nq");
+  if (nx == 0) return GB_OK;
+  GB_REQUIRE(c_xM && a_xG, "gb_lfc_add_k: null array");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t per = nx / nk;
+  if (dtype == GB_DTYPE_C128) return add_t<double2>(l, c_xM, a_xG, nx, 0, st, per);
+  return add_t<float2>(l, c_xM, a_xG, nx, 0, st, per);
+}
+
+int gb_lfc_integrate_k(const gb_lfc* l, const void* a_xG, void* c_xM, int64_t nx, int dtype, int nk,
+                       void* stream) {
+  GB_REQUIRE(l && dtype_valid(dtype) && nx >= 0, "gb_lfc_integrate_k: bad arguments");
+  GB_REQUIRE(dtype_complex(dtype), "gb_lfc_integrate_k: k-point batches are complex");
+  GB_REQUIRE(nk >= 1 && nk <= l->nq && nx % nk == 0,
+             "gb_lfc_integrate_k: nk must divide the batch and be <= nq");
+  if (nx == 0) return GB_OK;
+  GB_REQUIRE(c_xM && a_xG, "gb_lfc_integrate_k: null array");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t per = nx / nk;
+  if (dtype == GB_DTYPE_C128) return integrate_t<double2>(l, a_xG, c_xM, nx, 0, st, per);
+  return integrate_t<float2>(l, a_xG, c_xM, nx, 0, st, per);
 }
 
 int gb_lfc_derivative(const gb_lfc* l, const void* a_xG, void* c_xMv, int64_t nx, const double h_cv[9],

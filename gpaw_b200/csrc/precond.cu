@@ -29,12 +29,13 @@ static bool same3(const int64_t* a, const int64_t* b) {
   return a[0] == b[0] && a[1] == b[1] && a[2] == b[2];
 }
 
-extern "C" int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* rest1,
-                             const gb_transformer* intp1, const gb_transformer* intp2,
-                             const gb_operator* kin0, const gb_operator* kin1, const gb_operator* kin2,
-                             void* d0, void* q0, void* r1, void* d1, void* q1, void* r2, void* d2,
-                             void* q2, const void* residuals, const void* nresiduals, double step,
-                             int64_t nin, int dtype, const double* phase_cd, void* stream) {
+// the V-cycle with nk phase sets (one per equal group of bands)
+static int fd_precond_sets(const gb_transformer* rest0, const gb_transformer* rest1,
+                           const gb_transformer* intp1, const gb_transformer* intp2,
+                           const gb_operator* kin0, const gb_operator* kin1, const gb_operator* kin2,
+                           void* d0, void* q0, void* r1, void* d1, void* q1, void* r2, void* d2,
+                           void* q2, const void* residuals, const void* nresiduals, double step,
+                           int64_t nin, int dtype, const double* phase_cd, int nk, void* stream) {
   (void)q2;
   (void)nresiduals;
   GB_REQUIRE(rest0 && rest1 && intp1 && intp2 && kin0 && kin1 && kin2,
@@ -43,6 +44,7 @@ extern "C" int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* 
   if (nin == 0) return GB_OK;
   GB_REQUIRE(d0 && q0 && r1 && d1 && q1 && r2 && d2 && residuals, "gb_fd_precond: null work array");
   GB_REQUIRE(!dtype_complex(dtype) || phase_cd, "gb_fd_precond: complex data needs phase_cd");
+  GB_REQUIRE(nk >= 1 && nk <= KMAX && nin % nk == 0, "gb_fd_precond: bad number of k-point phase sets");
   GB_REQUIRE(!rest0->interpolate && !rest1->interpolate && intp1->interpolate && intp2->interpolate,
              "gb_fd_precond: transformer kinds do not match (rest0, rest1, intp1, intp2)");
   // level geometry must chain: kin0 on level 0, kin1 on level 1, kin2 on level 2
@@ -61,16 +63,36 @@ extern "C" int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* 
   int rc;
   Epilogue ep;
 
-  if ((rc = tr_apply(rest0, residuals, r1, nin, dtype, ph, st, -1.0, nullptr, 0.0))) return rc;
+  if ((rc = tr_apply(rest0, residuals, r1, nin, dtype, ph, st, -1.0, nullptr, 0.0, nk))) return rc;
   ep = Epilogue(); ep.alpha = 4 * s; ep.beta = -1.0;
-  if ((rc = op_apply(kin1, r1, q1, nin, dtype, ph, st, ep))) return rc;
-  if ((rc = tr_apply(rest1, q1, r2, nin, dtype, ph, st, 1.0, nullptr, 0.0))) return rc;
+  if ((rc = op_apply(kin1, r1, q1, nin, dtype, ph, st, ep, nk))) return rc;
+  if ((rc = tr_apply(rest1, q1, r2, nin, dtype, ph, st, 1.0, nullptr, 0.0, nk))) return rc;
   ep = Epilogue(); ep.alpha = -256.0 * s * s; ep.beta = 32.0 * s;
-  if ((rc = op_apply(kin2, r2, d2, nin, dtype, ph, st, ep))) return rc;
-  if ((rc = tr_apply(intp2, d2, d1, nin, dtype, ph, st, -1.0, r1, 4 * s))) return rc;
+  if ((rc = op_apply(kin2, r2, d2, nin, dtype, ph, st, ep, nk))) return rc;
+  if ((rc = tr_apply(intp2, d2, d1, nin, dtype, ph, st, -1.0, r1, 4 * s, nk))) return rc;
   ep = Epilogue(); ep.alpha = -4 * s; ep.beta = 1.0; ep.gamma = 4 * s; ep.y = r1;
-  if ((rc = op_apply(kin1, d1, q1, nin, dtype, ph, st, ep))) return rc;
-  if ((rc = tr_apply(intp1, q1, q0, nin, dtype, ph, st, -1.0, nullptr, 0.0))) return rc;
+  if ((rc = op_apply(kin1, d1, q1, nin, dtype, ph, st, ep, nk))) return rc;
+  if ((rc = tr_apply(intp1, q1, q0, nin, dtype, ph, st, -1.0, nullptr, 0.0, nk))) return rc;
   ep = Epilogue(); ep.alpha = s; ep.beta = -1.0; ep.gamma = -s; ep.y = residuals;
-  return op_apply(kin0, q0, d0, nin, dtype, ph, st, ep);
+  return op_apply(kin0, q0, d0, nin, dtype, ph, st, ep, nk);
+}
+
+extern "C" int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* rest1,
+                             const gb_transformer* intp1, const gb_transformer* intp2,
+                             const gb_operator* kin0, const gb_operator* kin1, const gb_operator* kin2,
+                             void* d0, void* q0, void* r1, void* d1, void* q1, void* r2, void* d2,
+                             void* q2, const void* residuals, const void* nresiduals, double step,
+                             int64_t nin, int dtype, const double* phase_cd, void* stream) {
+  return fd_precond_sets(rest0, rest1, intp1, intp2, kin0, kin1, kin2, d0, q0, r1, d1, q1, r2, d2, q2,
+                         residuals, nresiduals, step, nin, dtype, phase_cd, 1, stream);
+}
+
+extern "C" int gb_fd_precond_k(const gb_transformer* rest0, const gb_transformer* rest1,
+                               const gb_transformer* intp1, const gb_transformer* intp2,
+                               const gb_operator* kin0, const gb_operator* kin1, const gb_operator* kin2,
+                               void* d0, void* q0, void* r1, void* d1, void* q1, void* r2, void* d2,
+                               void* q2, const void* residuals, double step, int64_t nin, int dtype,
+                               int nk, const double* phase_kcd, void* stream) {
+  return fd_precond_sets(rest0, rest1, intp1, intp2, kin0, kin1, kin2, d0, q0, r1, d1, q1, r2, d2, q2,
+                         residuals, nullptr, step, nin, dtype, phase_kcd, nk, stream);
 }

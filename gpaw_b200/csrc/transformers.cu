@@ -37,9 +37,8 @@ struct TrArgs {
   int cbeg[3];        // interpolation coarse begin
   int tiles1, tiles2;
   int nsteps;         // marching steps along axis 0 per column
-  int has_phase;
   double alpha, gamma;
-  double ph[3][2][2];
+  PhaseSets phs;      // Bloch phases per k-point group of bands
   double w[4];        // midpoint weights for pairs at distance 1/2, 3/2, ...
 };
 
@@ -94,16 +93,16 @@ __device__ __forceinline__ void stage_plane(T* P, const T* S, int ry0, int cx0, 
 // multiply wrapped cells of a staged plane by the Bloch phase
 template <typename T, int NR, int NC, int PITCH, int NT>
 __device__ __forceinline__ void phase_fixup(T* P, int ry0, int cx0, int n1, int n2,
-                                            const TrArgs& a, int tid) {
+                                            const TrArgs& a, const double (&PH)[3][2][2], int tid) {
   for (int e = tid; e < NR * NC; e += NT) {
     const int r = e / NC, c = e % NC;
     const int y = ry0 + r, z = cx0 + c;
     double pr = 1.0, pi = 0.0;
     bool w = false;
-    if (a.pbc[1] && (y < 0 || y >= n1)) { const int s = y < 0; pr = a.ph[1][s][0]; pi = a.ph[1][s][1]; w = true; }
+    if (a.pbc[1] && (y < 0 || y >= n1)) { const int s = y < 0; pr = PH[1][s][0]; pi = PH[1][s][1]; w = true; }
     if (a.pbc[2] && (z < 0 || z >= n2)) {
       const int s = z < 0;
-      const double qr = a.ph[2][s][0], qi = a.ph[2][s][1];
+      const double qr = PH[2][s][0], qi = PH[2][s][1];
       const double tr = pr * qr - pi * qi, ti = pr * qi + pi * qr;
       pr = tr; pi = ti; w = true;
     }
@@ -163,6 +162,7 @@ __global__ void __launch_bounds__(C::NT) restrict_kernel(const TrArgs a) {
     const int Y0 = (t / a.tiles2) * CY, Z0 = (t % a.tiles2) * CZ;
     const T* src = reinterpret_cast<const T*>(a.in) + band * nf12 * nf0;
     T* dst = reinterpret_cast<T*>(a.out) + band * nc12 * nc0;
+    const auto& PH = a.phs.ph[phase_set_of(a.phs, band)];
     const int ry0 = 2 * Y0 + a.off[1] - (K - 1);
     const int s0 = 2 * Z0 + a.off[2] - (K - 1);
     const int cx0 = floor_div(s0, VEC) * VEC;
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(C::NT) restrict_kernel(const TrArgs a) {
       if (j >= 0 && j < nf0) return j;
       if (!a.pbc[0]) return -1;
       const int sd = j < 0;
-      pr = a.ph[0][sd][0]; pi = a.ph[0][sd][1];
+      pr = PH[0][sd][0]; pi = PH[0][sd][1];
       return tr_mod(j, nf0);
     };
     auto issue = [&](int j) {
@@ -203,8 +203,8 @@ __global__ void __launch_bounds__(C::NT) restrict_kernel(const TrArgs a) {
       T* P = ring + ((j - j0) % NS) * PLANE;
       T u = zero<T>();
       if (sp >= 0) {
-        if (CPLX && a.has_phase && edge) {
-          phase_fixup<T, FR, PITCH, PITCH, NT>(P, ry0, cx0, nf1, nf2, a, tid);
+        if (CPLX && a.phs.any && edge) {
+          phase_fixup<T, FR, PITCH, PITCH, NT>(P, ry0, cx0, nf1, nf2, a, PH, tid);
           __syncthreads();
         }
         if constexpr (K == 2) {
@@ -320,6 +320,7 @@ __global__ void __launch_bounds__(C::NT) interpolate_kernel(const TrArgs a) {
     const int Y0 = (t / a.tiles2) * FY, Z0 = (t % a.tiles2) * FZ;
     const T* src = reinterpret_cast<const T*>(a.in) + band * nc12 * nc0;
     T* dst = reinterpret_cast<T*>(a.out) + band * nf12 * nf0;
+    const auto& PH = a.phs.ph[phase_set_of(a.phs, band)];
     const T* ysrc = a.y ? reinterpret_cast<const T*>(a.y) + band * nf12 * nf0 : nullptr;
     // coarse rows / cols staged: global coarse index base, local = global - cbeg
     const int crow0 = floor_div(Y0 + a.skip0[1], 2) - (KH - 1);          // global coarse row of staged row 0
@@ -338,7 +339,7 @@ __global__ void __launch_bounds__(C::NT) interpolate_kernel(const TrArgs a) {
       if (l >= 0 && l < nc0) return l;
       if (!a.pbc[0]) return -1;
       const int sd = l < 0;
-      pr = a.ph[0][sd][0]; pi = a.ph[0][sd][1];
+      pr = PH[0][sd][0]; pi = PH[0][sd][1];
       return tr_mod(l, nc0);
     };
     auto issue = [&](int g) {
@@ -369,8 +370,8 @@ __global__ void __launch_bounds__(C::NT) interpolate_kernel(const TrArgs a) {
       T* P = ring + ((g - g0) % NS) * PLANE;
       T u[RY][RZ];
       if (sp >= 0) {
-        if (CPLX && a.has_phase && edge) {
-          phase_fixup<T, CR, PITCH, PITCH, NT>(P, ry0, cx0, nc1, nc2, a, tid);
+        if (CPLX && a.phs.any && edge) {
+          phase_fixup<T, CR, PITCH, PITCH, NT>(P, ry0, cx0, nc1, nc2, a, PH, tid);
           __syncthreads();
         }
         // pass A: along axis 2, every staged coarse row -> FZ fine columns
@@ -485,7 +486,7 @@ static void midpoint_weights(int k, double* w) {
   }
 }
 
-static void fill_common(const gb_transformer* t, TrArgs& a, const double* ph) {
+static void fill_common(const gb_transformer* t, TrArgs& a, const double* ph, int nk, int64_t nbatch) {
   memset(&a, 0, sizeof(a));
   for (int c = 0; c < 3; ++c) {
     a.ni[c] = (int)t->nin_c[c];
@@ -496,12 +497,7 @@ static void fill_common(const gb_transformer* t, TrArgs& a, const double* ph) {
     a.cbeg[c] = t->cbeg[c];
   }
   midpoint_weights(t->k, a.w);
-  for (int c = 0; c < 3; ++c)
-    for (int d = 0; d < 2; ++d) {
-      a.ph[c][d][0] = ph ? ph[(c * 2 + d) * 2] : 1.0;
-      a.ph[c][d][1] = ph ? ph[(c * 2 + d) * 2 + 1] : 0.0;
-      if (a.ph[c][d][0] != 1.0 || a.ph[c][d][1] != 0.0) a.has_phase = 1;
-    }
+  fill_phase_sets(a.phs, ph, nk, nbatch);
 }
 
 template <class C, typename KernelT>
@@ -524,10 +520,10 @@ static int launch_persistent(KernelT kernel, const TrArgs& a, int64_t total, cud
 
 template <typename T, int K, int CY, int CZ>
 static int restrict_cfg(const gb_transformer* t, const void* in, void* out, int64_t nin,
-                        const double* ph, cudaStream_t st, double alpha) {
+                        const double* ph, cudaStream_t st, double alpha, int nk) {
   using C = RCfg<T, K, CY, CZ, 2>;
   TrArgs a;
-  fill_common(t, a, ph);
+  fill_common(t, a, ph, nk, nin);
   a.in = in; a.out = out; a.nbatch = nin; a.alpha = alpha;
   a.tiles1 = ceil_div(a.no[1], C::CY);
   a.tiles2 = ceil_div(a.no[2], C::CZ);
@@ -621,7 +617,7 @@ static int restrict2_march_launch(const gb_transformer* t, const void* in, void*
                                   cudaStream_t st, double alpha) {
   constexpr int VEC = 16 / (int)sizeof(T);
   TrArgs a;
-  fill_common(t, a, nullptr);
+  fill_common(t, a, nullptr, 1, nin);
   a.in = in; a.out = out; a.nbatch = nin; a.alpha = alpha;
   const int ngx = (a.no[2] + 1) / 2;
   const int TYC = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
@@ -766,7 +762,7 @@ static int interp2_march_launch(const gb_transformer* t, const void* in, void* o
                                 cudaStream_t st, double alpha, const void* y, double gamma) {
   constexpr int VEC = 16 / (int)sizeof(T);
   TrArgs a;
-  fill_common(t, a, nullptr);
+  fill_common(t, a, nullptr, 1, nin);
   a.in = in; a.out = out; a.nbatch = nin; a.alpha = alpha; a.y = y; a.gamma = gamma;
   const int ngx = a.no[2] / 4;
   const int TYF = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
@@ -784,24 +780,25 @@ static int interp2_march_launch(const gb_transformer* t, const void* in, void* o
 // 16 x 16 tile, wider ones 8 x 32: no more than half a warp idles on a row
 template <typename T, int K>
 static int restrict_k(const gb_transformer* t, const void* in, void* out, int64_t nin,
-                      const double* ph, cudaStream_t st, double alpha) {
+                      const double* ph, cudaStream_t st, double alpha, int nk) {
   if constexpr (K == 2 && !Elem<T>::cplx) {
     if (restrict2_march_ok<T>(t, nin, ph)) return restrict2_march_launch<T>(t, in, out, nin, st, alpha);
   }
-  if (t->nout_c[2] <= 16) return restrict_cfg<T, K, 16, 16>(t, in, out, nin, ph, st, alpha);
-  return restrict_cfg<T, K, 8, 32>(t, in, out, nin, ph, st, alpha);
+  if (t->nout_c[2] <= 16) return restrict_cfg<T, K, 16, 16>(t, in, out, nin, ph, st, alpha, nk);
+  return restrict_cfg<T, K, 8, 32>(t, in, out, nin, ph, st, alpha, nk);
 }
 
 template <typename T, int K>
 static int interpolate_k(const gb_transformer* t, const void* in, void* out, int64_t nin,
-                         const double* ph, cudaStream_t st, double alpha, const void* y, double gamma) {
+                         const double* ph, cudaStream_t st, double alpha, const void* y, double gamma,
+                         int nk) {
   if constexpr (K == 2 && !Elem<T>::cplx) {
     if (interp2_march_ok<T>(t, nin, ph, y)) return interp2_march_launch<T>(t, in, out, nin, st, alpha, y, gamma);
   }
   constexpr int RZ = sizeof(T) == 4 ? 4 : (sizeof(T) == 8 ? 2 : 1);
   using C = ICfg<T, K, 16, 32, 2, RZ, 2>;
   TrArgs a;
-  fill_common(t, a, ph);
+  fill_common(t, a, ph, nk, nin);
   a.in = in; a.out = out; a.nbatch = nin; a.alpha = alpha; a.y = y; a.gamma = gamma;
   a.tiles1 = ceil_div(a.no[1], C::FY);
   a.tiles2 = ceil_div(a.no[2], C::FZ);
@@ -815,31 +812,34 @@ static int interpolate_k(const gb_transformer* t, const void* in, void* out, int
 
 template <typename T>
 static int tr_dispatch(const gb_transformer* t, const void* in, void* out, int64_t nin,
-                       const double* ph, cudaStream_t st, double alpha, const void* y, double gamma) {
+                       const double* ph, cudaStream_t st, double alpha, const void* y, double gamma,
+                       int nk) {
   if (t->interpolate) {
     switch (t->k) {
-      case 2: return interpolate_k<T, 2>(t, in, out, nin, ph, st, alpha, y, gamma);
-      case 4: return interpolate_k<T, 4>(t, in, out, nin, ph, st, alpha, y, gamma);
-      case 6: return interpolate_k<T, 6>(t, in, out, nin, ph, st, alpha, y, gamma);
-      default: return interpolate_k<T, 8>(t, in, out, nin, ph, st, alpha, y, gamma);
+      case 2: return interpolate_k<T, 2>(t, in, out, nin, ph, st, alpha, y, gamma, nk);
+      case 4: return interpolate_k<T, 4>(t, in, out, nin, ph, st, alpha, y, gamma, nk);
+      case 6: return interpolate_k<T, 6>(t, in, out, nin, ph, st, alpha, y, gamma, nk);
+      default: return interpolate_k<T, 8>(t, in, out, nin, ph, st, alpha, y, gamma, nk);
     }
   }
   if (y) return fail(GB_E_UNSUPPORTED, "restriction has no y epilogue");
   switch (t->k) {
-    case 2: return restrict_k<T, 2>(t, in, out, nin, ph, st, alpha);
-    case 4: return restrict_k<T, 4>(t, in, out, nin, ph, st, alpha);
-    case 6: return restrict_k<T, 6>(t, in, out, nin, ph, st, alpha);
-    default: return restrict_k<T, 8>(t, in, out, nin, ph, st, alpha);
+    case 2: return restrict_k<T, 2>(t, in, out, nin, ph, st, alpha, nk);
+    case 4: return restrict_k<T, 4>(t, in, out, nin, ph, st, alpha, nk);
+    case 6: return restrict_k<T, 6>(t, in, out, nin, ph, st, alpha, nk);
+    default: return restrict_k<T, 8>(t, in, out, nin, ph, st, alpha, nk);
   }
 }
 
 int tr_apply(const gb_transformer* t, const void* in, void* out, int64_t nin, int dtype,
-             const double* ph, cudaStream_t st, double alpha, const void* y, double gamma) {
+             const double* ph, cudaStream_t st, double alpha, const void* y, double gamma, int nk) {
+  if (nk > KMAX) return fail(GB_E_UNSUPPORTED, "more k-point phase sets than one launch takes");
+  if (nk > 1 && nin % nk) return fail(GB_E_INVALID, "batch not divisible by the number of phase sets");
   switch (dtype) {
-    case GB_DTYPE_F64: return tr_dispatch<double>(t, in, out, nin, ph, st, alpha, y, gamma);
-    case GB_DTYPE_F32: return tr_dispatch<float>(t, in, out, nin, ph, st, alpha, y, gamma);
-    case GB_DTYPE_C128: return tr_dispatch<double2>(t, in, out, nin, ph, st, alpha, y, gamma);
-    default: return tr_dispatch<float2>(t, in, out, nin, ph, st, alpha, y, gamma);
+    case GB_DTYPE_F64: return tr_dispatch<double>(t, in, out, nin, ph, st, alpha, y, gamma, nk);
+    case GB_DTYPE_F32: return tr_dispatch<float>(t, in, out, nin, ph, st, alpha, y, gamma, nk);
+    case GB_DTYPE_C128: return tr_dispatch<double2>(t, in, out, nin, ph, st, alpha, y, gamma, nk);
+    default: return tr_dispatch<float2>(t, in, out, nin, ph, st, alpha, y, gamma, nk);
   }
 }
 
@@ -929,6 +929,18 @@ int gb_transformer_apply_axpy(const gb_transformer* t, const void* in, void* out
 int gb_transformer_free(gb_transformer* t) {
   delete t;
   return GB_OK;
+}
+
+int gb_transformer_apply_k(const gb_transformer* t, const void* in, void* out, int64_t nin, int dtype, int nk,
+                           const double* phase_kcd, void* stream) {
+  GB_REQUIRE(t && dtype_valid(dtype) && nin >= 0, "gb_transformer_apply_k: bad arguments");
+  GB_REQUIRE(dtype_complex(dtype) == !t->real, "gb_transformer_apply_k: dtype does not match the transformer");
+  GB_REQUIRE(nk >= 1 && nk <= KMAX && nin % nk == 0, "gb_transformer_apply_k: bad number of phase sets");
+  if (nin == 0) return GB_OK;
+  GB_REQUIRE(in && out && in != out, "gb_transformer_apply_k: bad data pointers");
+  GB_REQUIRE(!dtype_complex(dtype) || phase_kcd, "gb_transformer_apply_k: complex data needs phases");
+  return tr_apply(t, in, out, nin, dtype, dtype_complex(dtype) ? phase_kcd : nullptr, (cudaStream_t)stream, 1.0,
+                  nullptr, 0.0, nk);
 }
 
 }  // extern "C"

@@ -50,6 +50,8 @@ class Eigensolver:
         reference's default 'occupied' band convergence)."""
         w = getattr(kpt, '_w_n', None)
         if w is None:
+            # kpt.weight: the k-point weight (an array of one per row for a
+            # k-point batch)
             w = torch.as_tensor(np.where(np.asarray(kpt.f_n) > 0, kpt.weight, 0.0),
                                 dtype=torch.float64, device=kpt.psit_nG.device)
             kpt._w_n = w
@@ -70,22 +72,37 @@ class Eigensolver:
 
     def subspace_matrix(self, ham, wfs, kpt):
         """(H_nn in FP64, (T + v) psi): everything before the eigensolver of
-        the subspace problem (no host synchronisation)."""
+        the subspace problem (no host synchronisation); for a k-point batch
+        H is (nk, nbands, nbands), one block per k-point."""
         psit = kpt.psit_nG
+        nk = getattr(kpt, 'nk', 1)
         Htpsit = torch.empty_like(psit)
         wfs.apply_pseudo_hamiltonian(kpt, ham, psit, Htpsit)
-        H = wfs.matrix(psit, Htpsit)
+        H = wfs.matrix(psit, Htpsit, nk)
         wide = torch.complex128 if wfs.dtype.is_complex else torch.float64
         if kpt.P_nM is not None and kpt.P_nM.shape[-1]:
             Pw = kpt.P_nM.to(wide)
-            H = H + (Pw.conj() @ ham.dH_MM.to(wide)) @ Pw.T
-        H = 0.5 * (H + H.conj().T)
+            if nk > 1:
+                Pw = Pw.reshape(nk, Pw.shape[0] // nk, -1)
+            H = H + (Pw.conj() @ ham.dH_MM.to(wide)) @ Pw.transpose(-1, -2)
+        H = 0.5 * (H + H.conj().transpose(-1, -2))
         return H, Htpsit
 
     def subspace_rotate(self, wfs, kpt, eps, V, Htpsit):
-        """psi, (T + v) psi and P rotated to the eigenvectors V of H_nn."""
+        """psi, (T + v) psi and P rotated to the eigenvectors V of H_nn
+        (per k-point for a batch: V (nk, nbands, nbands), eps flattened)."""
         psit = kpt.psit_nG
         nb = psit.shape[0]
+        nk = getattr(kpt, 'nk', 1)
+        if nk > 1:
+            U = V.transpose(1, 2).to(wfs.dtype)
+            rot = lambda x: torch.bmm(U, x.reshape(nk, nb // nk, -1)).reshape(x.shape)
+            kpt.psit_nG = rot(psit)
+            self.Htpsit_nG = rot(Htpsit)
+            if kpt.P_nM is not None:
+                kpt.P_nM = rot(kpt.P_nM)
+            kpt.eps_n = eps.reshape(-1)
+            return
         # phi_k = sum_m V[m, k] psi_m
         if psit.dtype == torch.float32:
             # FP32 real: tensor-core rotations sharing one TF32 split of
@@ -111,5 +128,5 @@ class Eigensolver:
 
     def subspace_diagonalize(self, ham, wfs, kpt):
         H, Htpsit = self.subspace_matrix(ham, wfs, kpt)
-        eps, V = torch.linalg.eigh(H)
+        eps, V = torch.linalg.eigh(H)          # batched over k for a batch
         self.subspace_rotate(wfs, kpt, eps, V, Htpsit)

@@ -132,10 +132,22 @@ class FDOperator:
         if in_xg.dtype.is_complex and phase_cd is None:
             phase_cd = np.ones((3, 2), complex)
         nin = int(np.prod(in_xg.shape[:-3], dtype=np.int64))
+        if in_xg.dtype.is_complex and nat.is_phase_batch(phase_cd):
+            return self._apply_k(in_xg, out_xg, nin, phase_cd, None)
         nat.check(nat.lib().gb_operator_apply(
             self._handle, nat.ptr(in_xg), nat.ptr(out_xg), nin,
             nat.dtype_code(in_xg), nat.phases(phase_cd) if in_xg.dtype.is_complex
             else None, nat.stream_of(in_xg)), 'gb_operator_apply')
+        return out_xg
+
+    def _apply_k(self, in_xg, out_xg, nin, phase_kcd, vt_g):
+        """A k-point batch: leading dims hold nk equal groups of grids,
+        group k with the Bloch phases phase_kcd[k] (one launch)."""
+        nk, ph = nat.phase_sets(phase_kcd)
+        nat.check(nat.lib().gb_operator_apply_k(
+            self._handle, nat.ptr(in_xg), nat.ptr(out_xg), nin, nat.dtype_code(in_xg), nk,
+            ph, nat.ptr(vt_g) if vt_g is not None else None, nat.stream_of(in_xg)),
+            'gb_operator_apply_k')
         return out_xg
 
     def apply_potential(self, in_xg, out_xg, vt_g, phase_cd=None):
@@ -152,6 +164,8 @@ class FDOperator:
         if in_xg.dtype.is_complex and phase_cd is None:
             phase_cd = np.ones((3, 2), complex)
         nin = int(np.prod(in_xg.shape[:-3], dtype=np.int64))
+        if in_xg.dtype.is_complex and nat.is_phase_batch(phase_cd):
+            return self._apply_k(in_xg, out_xg, nin, phase_cd, vt_g)
         nat.check(nat.lib().gb_operator_apply_potential(
             self._handle, nat.ptr(in_xg), nat.ptr(out_xg), nin, nat.dtype_code(in_xg),
             nat.ptr(vt_g), nat.phases(phase_cd) if in_xg.dtype.is_complex else None,

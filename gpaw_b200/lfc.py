@@ -329,6 +329,12 @@ class LocalizedFunctionsCollection(BaseLFC):
             return -1
         return q
 
+    @staticmethod
+    def _kbatch(q):
+        """q = range(nk): the rows are nk equal groups, group k at k-point
+        q = k (one launch for the batch); returns nk, or 0 for a single q."""
+        return len(q) if isinstance(q, range) else 0
+
     # -- reference interface --------------------------------------------------
     def add(self, a_xG, c_axi=1.0, q=-1):
         """a_xG += sum_a,i c_axi Phi^a_i (gpaw/lfc.py:392-472)."""
@@ -356,6 +362,13 @@ class LocalizedFunctionsCollection(BaseLFC):
             return
         nx = int(np.prod(tuple(a_xG.shape[:-3]), dtype=np.int64))
         c_xM = c_xM.to(a_xG.dtype).contiguous()
+        nk = self._kbatch(q)
+        if nk:
+            assert q.start == 0 and q.step == 1
+            nat.check(nat.lib().gb_lfc_add_k(
+                self.lfc.handle, nat.ptr(c_xM), nat.ptr(a_xG), nx,
+                nat.dtype_code(a_xG), nk, nat.stream_of(a_xG)), 'gb_lfc_add_k')
+            return
         nat.check(nat.lib().gb_lfc_add(
             self.lfc.handle, nat.ptr(c_xM), nat.ptr(a_xG), nx,
             nat.dtype_code(a_xG), self._nq(a_xG, q), nat.stream_of(a_xG)),
@@ -369,10 +382,17 @@ class LocalizedFunctionsCollection(BaseLFC):
         nx = int(np.prod(xshape, dtype=np.int64))
         if self.Mmax == 0:
             return c_xM
-        nat.check(nat.lib().gb_lfc_integrate(
-            self.lfc.handle, nat.ptr(a_xG), nat.ptr(c_xM), nx,
-            nat.dtype_code(a_xG), self._nq(a_xG, q), nat.stream_of(a_xG)),
-            'gb_lfc_integrate')
+        nk = self._kbatch(q)
+        if nk:
+            assert q.start == 0 and q.step == 1
+            nat.check(nat.lib().gb_lfc_integrate_k(
+                self.lfc.handle, nat.ptr(a_xG), nat.ptr(c_xM), nx,
+                nat.dtype_code(a_xG), nk, nat.stream_of(a_xG)), 'gb_lfc_integrate_k')
+        else:
+            nat.check(nat.lib().gb_lfc_integrate(
+                self.lfc.handle, nat.ptr(a_xG), nat.ptr(c_xM), nx,
+                nat.dtype_code(a_xG), self._nq(a_xG, q), nat.stream_of(a_xG)),
+                'gb_lfc_integrate')
         for a in self.my_atom_indices:
             if a in c_axi:
                 M1 = self.M_a[a]

@@ -72,6 +72,17 @@ class Preconditioner:
         r1, d1, q1 = w1
         r2, d2, q2 = w2
         P = nat.ptr
+        if residuals.dtype.is_complex and nat.is_phase_batch(phases):
+            # a k-point batch: nk equal groups of bands, one phase set each
+            nk, ph = nat.phase_sets(phases)
+            nat.check(nat.lib().gb_fd_precond_k(
+                self.restrictor_object0.handle, self.restrictor_object1.handle,
+                self.interpolator_object1.handle, self.interpolator_object2.handle,
+                self.kin0.handle, self.kin1.handle, self.kin2.handle,
+                P(out), P(q0), P(r1), P(d1), P(q1), P(r2), P(d2), P(q2),
+                P(residuals), self.step, nb, nat.dtype_code(residuals), nk, ph,
+                nat.stream_of(residuals)), 'gb_fd_precond_k')
+            return out
         nat.check(nat.lib().gb_fd_precond(
             self.restrictor_object0.handle, self.restrictor_object1.handle,
             self.interpolator_object1.handle, self.interpolator_object2.handle,

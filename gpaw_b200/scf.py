@@ -153,7 +153,8 @@ class Calculation:
     def __init__(self, symbols, positions, cell, pbc, h=0.2, nbands=None,
                  xc='LDA', precision='fp64', k_c=None, preconditioner=None,
                  mixer_beta=None, seed=0, device='cuda', stencil=3,
-                 r_gauss=0.6, kerker_q0=1.0, blocksize=None):
+                 r_gauss=0.6, kerker_q0=1.0, blocksize=None, kpts=None,
+                 kbatch=True):
         cell = np.array(cell, float)
         cell_cv = np.diag(cell) if cell.ndim == 1 else cell
         self.cell_cv = cell_cv / Bohr
@@ -171,7 +172,20 @@ class Calculation:
         nocc = self.nvalence // 2
         self.nbands = nbands or max(nocc + 4, int(1.2 * nocc))
         self.precision = precision
-        cplx = k_c is not None and np.any(k_c)
+        # k-points: a Monkhorst-Pack grid reduced by time reversal, one given
+        # k-point, or Gamma
+        if kpts is not None:
+            self.ibz_kc, self.w_k = irreducible_kpoints(monkhorst_pack(kpts))
+        elif k_c is not None:
+            self.ibz_kc, self.w_k = np.array([k_c], float), np.ones(1)
+        else:
+            self.ibz_kc, self.w_k = np.zeros((1, 3)), np.ones(1)
+        # kbatch: every k-point in each launch (one batched KPoint); else one
+        # KPoint per k-point, iterated in turn as the reference does
+        self.kbatch = kbatch and len(self.ibz_kc) > 1
+        if self.kbatch and blocksize is not None:
+            raise ValueError('a k-point batch runs every band in one block (blocksize=None)')
+        cplx = bool(np.any(self.ibz_kc))
         if precision == 'fp64':
             dtype = torch.complex128 if cplx else torch.float64
         else:
@@ -182,7 +196,7 @@ class Calculation:
             class _KD:
                 pass
             kd = _KD()
-            kd.ibzk_qc = np.array([k_c], float)
+            kd.ibzk_qc = self.ibz_kc
             kd.gamma = False
         self.wfs = FDWaveFunctions(self.gd, self.nbands, self.setups, self.spos_ac,
                                    dtype, stencil, kd)
@@ -212,7 +226,7 @@ class Calculation:
             self.gd, self.wfs.kin, complex if cplx else float, block=10)
         self.eigensolver.initialize(self.wfs, self.preconditioner)
         self.seed = seed
-        self.k_c = np.zeros(3) if k_c is None else np.asarray(k_c, float)
+        self.k_c = self.ibz_kc[0]
         self.vHt_g = self.finegd.zeros()
         self.dH_MM = None
         self.e_constant = self._constant_energy()
@@ -234,26 +248,41 @@ class Calculation:
         lfc.set_positions(self.spos_ac)
         rng = np.random.default_rng(self.seed)
         M = lfc.Mmax
-        c = rng.standard_normal((self.nbands, M))
-        if cplx:
-            c = c + 0.1j * rng.standard_normal(c.shape)
         work = torch.complex128 if cplx else torch.float64
-        psit = self.gd.zeros(self.nbands, dtype=work)
-        c_axi = {a: torch.from_numpy(c[:, lfc.M_a[a]:lfc.M_a[a] + 4].copy()).to(
-            self.gd.device, work) for a in range(len(self.setups))}
-        lfc.add(psit, c_axi, 0 if cplx else -1)
+        nk = len(self.ibz_kc)
+        psit = self.gd.zeros(nk * self.nbands, dtype=work)
+        for k in range(nk):
+            c = rng.standard_normal((self.nbands, M))
+            if cplx:
+                c = c + 0.1j * rng.standard_normal(c.shape)
+            c_axi = {a: torch.from_numpy(c[:, lfc.M_a[a]:lfc.M_a[a] + 4].copy()).to(
+                self.gd.device, work) for a in range(len(self.setups))}
+            part = psit[k * self.nbands:(k + 1) * self.nbands]
+            lfc.add(part, c_axi, k if cplx else -1)
         # a little noise so that the start spans more than nbands' worth of LCAO space
         gen = torch.Generator(device=self.gd.device).manual_seed(self.seed)
         noise = torch.randn(psit.shape, generator=gen, device=self.gd.device,
                             dtype=torch.float64)
         psit += 0.01 * noise * psit.abs().max()
-        phase = self.gd.phase_factor_cd(self.k_c) if cplx else None
-        kpt = KPoint(psit.to(self.dtype), q=0 if cplx else -1, phase_cd=phase,
-                     weight=1.0, k_c=self.k_c)
+        psit = psit.to(self.dtype)
         nocc = self.nvalence // 2
-        kpt.f_n = np.array([2.0] * nocc + [0.0] * (self.nbands - nocc))
-        self.wfs.kpt_u = [kpt]
-        self.wfs.orthonormalize(kpt)
+        occ = np.array([2.0] * nocc + [0.0] * (self.nbands - nocc))
+        phases = [self.gd.phase_factor_cd(k_c) if cplx else None for k_c in self.ibz_kc]
+        if self.kbatch:
+            kpt = KPoint(psit, q=range(nk), phase_cd=np.array(phases),
+                         weight=np.repeat(self.w_k, self.nbands), k_c=self.ibz_kc, nk=nk)
+            kpt.f_n = np.tile(occ, nk) * np.repeat(self.w_k, self.nbands)
+            self.wfs.kpt_u = [kpt]
+        else:
+            self.wfs.kpt_u = []
+            for k in range(nk):
+                kpt = KPoint(psit[k * self.nbands:(k + 1) * self.nbands].clone(),
+                             q=k if cplx else -1, phase_cd=phases[k], weight=self.w_k[k],
+                             k_c=self.ibz_kc[k])
+                kpt.f_n = occ * self.w_k[k]
+                self.wfs.kpt_u.append(kpt)
+        for kpt in self.wfs.kpt_u:
+            self.wfs.orthonormalize(kpt)
         self.wfs.orthonormalized = True
 
     def _init_density(self):
@@ -315,14 +344,16 @@ class Calculation:
                 dH[M:M + s.ni, M:M + s.ni] = torch.from_numpy(np.asarray(s.dH_ii, float))
         return dH.to(self.gd.device)
 
-    def total_energy(self, kpt):
+    def total_energy(self, kpt=None):
         """E = sum f eps - int nt vt + E_H + E_xc + E_vbar + E_0 (Hartree),
         all sums in FP64 (the band energy counts kinetic + nonlocal +
         local parts of the input potential); E_0 is the geometry constant
         of `_constant_energy`."""
-        if getattr(kpt, '_f_t', None) is None:
-            kpt._f_t = torch.as_tensor(np.asarray(kpt.f_n, float), device=self.gd.device)
-        band = (kpt._f_t * kpt.eps_n).sum()
+        band = 0.0
+        for k in (self.wfs.kpt_u if kpt is None or len(self.wfs.kpt_u) > 1 else [kpt]):
+            if getattr(k, '_f_t', None) is None:
+                k._f_t = torch.as_tensor(np.asarray(k.f_n, float), device=self.gd.device)
+            band = band + (k._f_t * k.eps_n).sum()
         nvt = (self.nt_G * self.vt_G).sum() * self.gd.dv
         return band - nvt + self.e_terms.sum() + self.e_constant
 
@@ -371,9 +402,8 @@ class Calculation:
         """One SCF iteration, eagerly: RMM-DIIS pass, energy, density mixing,
         new potential.  Returns the FP64 device vector [E (eV), eigenstate
         error, density change]."""
-        kpt = self.wfs.kpt_u[0]
         err = self.eigensolver.iterate(self, self.wfs)
-        E = self.total_energy(kpt) * Hartree
+        E = self.total_energy() * Hartree
         ddens = self.update_density()
         self.update_hamiltonian()
         return torch.stack([E, err, ddens, self._judge_flag()])
@@ -415,7 +445,7 @@ class Calculation:
         for it in range(1, maxiter + 1):
             if snap is not None:
                 snap.take()
-            if graph and self.mixer.count == self.mixer.nmaxold:
+            if graph and len(self.wfs.kpt_u) == 1 and self.mixer.count == self.mixer.nmaxold:
                 if step is None:
                     step = _GraphedIteration(self)
                 out = step.replay()
@@ -460,9 +490,14 @@ class Calculation:
         return log
 
     def eigenvalues(self):
-        eps = self.wfs.kpt_u[0].eps_n
-        eps = eps.cpu().numpy() if isinstance(eps, torch.Tensor) else np.asarray(eps)
-        return eps * Hartree
+        """eV: (nbands,) at Gamma / one k-point, (nk, nbands) otherwise."""
+        out = []
+        for kpt in self.wfs.kpt_u:
+            eps = kpt.eps_n
+            eps = eps.cpu().numpy() if isinstance(eps, torch.Tensor) else np.asarray(eps)
+            out.append(eps.reshape(-1, self.nbands))
+        eps = np.concatenate(out) * Hartree
+        return eps[0] if len(eps) == 1 else eps
 
     # -------------------------------------------------------------- forces
     def forces(self):
@@ -479,16 +514,23 @@ class Calculation:
           ion-ion        the geometry constant's gradient
         Device work in the precision of the run (sums in FP64); the small
         per-atom reductions on the host."""
-        kpt = self.wfs.kpt_u[0]
         natoms = len(self.setups)
         F = np.zeros((natoms, 3))
         pt = self.wfs.pt
-        f_n = torch.as_tensor(np.asarray(kpt.f_n, float), device=self.gd.device)
         if pt.Mmax:
-            D = pt.derivative(kpt.psit_nG, {}, kpt.q if self.dtype.is_complex else -1)
-            P = kpt.P_nM.to(torch.float64)
-            C = P @ self.dH_MM.T
-            F_Mv = 2 * (f_n[:, None, None] * D.to(torch.float64) * C[:, :, None]).sum(0)
+            F_Mv = torch.zeros((pt.Mmax, 3), dtype=torch.float64, device=self.gd.device)
+            wide = torch.complex128 if self.dtype.is_complex else torch.float64
+            for kpt in self.wfs.kpt_u:
+                f_n = torch.as_tensor(np.asarray(kpt.f_n, float), device=self.gd.device)
+                nk = getattr(kpt, 'nk', 1)
+                nb = kpt.psit_nG.shape[0] // nk
+                for k in range(nk):
+                    rows = slice(k * nb, (k + 1) * nb)
+                    q = (k if nk > 1 else kpt.q) if self.dtype.is_complex else -1
+                    D = pt.derivative(kpt.psit_nG[rows].contiguous(), {}, q).to(wide)
+                    C = kpt.P_nM[rows].to(wide) @ self.dH_MM.to(wide).T
+                    # 2 Re sum_n f_n conj(D_nMv) C_nM
+                    F_Mv += 2 * (f_n[rows, None, None] * (D.conj() * C[:, :, None]).real).sum(0)
             F_Mv = F_Mv.cpu().numpy()
             for a in range(natoms):
                 M = pt.M_a[a]
@@ -545,6 +587,31 @@ class Calculation:
             # E_0 = 1/2 sum_ab phi(|R_b + n - R_a|): d/dR_a picks both ends
             G -= (dphi[:, :, None] * d / R[:, :, None]).sum(1)
         return G
+
+
+def monkhorst_pack(size):
+    """The Monkhorst-Pack grid of size n1 x n2 x n3 (scaled k-points),
+    (i + 1/2) / n - 1/2 along each axis."""
+    size = np.asarray(size, int)
+    return (np.indices(size).reshape(3, -1).T + 0.5) / size - 0.5
+
+
+def irreducible_kpoints(k_kc, tol=1e-8):
+    """Reduce by time reversal only (psi_-k = psi_k^*, so k and -k give
+    the same density and energies): (ibz_kc, weights), weights summing to
+    one.  Point-group symmetry is not used."""
+    ibz, w = [], []
+    for k in k_kc:
+        for i, q in enumerate(ibz):
+            d = k + q
+            if np.all(np.abs(d - np.round(d)) < tol):
+                w[i] += 1
+                break
+        else:
+            ibz.append(np.array(k, float))
+            w.append(1)
+    w = np.array(w, float)
+    return np.array(ibz), w / w.sum()
 
 
 def si_diamond(ncell=1, a=5.43, rattle=0.0, seed=0):
@@ -698,9 +765,12 @@ class _GraphedIteration:
         self.psit = kpt.psit_nG
         self.P = kpt.P_nM
         nb = self.psit.shape[0]
+        nk = getattr(kpt, 'nk', 1)
         wide = torch.complex128 if wfs.dtype.is_complex else torch.float64
         self.eps = torch.empty(nb, dtype=torch.float64, device=self.psit.device)
-        self.V = torch.empty((nb, nb), dtype=wide, device=self.psit.device)
+        # one eigenvector block per k-point of a batch
+        vshape = (nk, nb // nk, nb // nk) if nk > 1 else (nb, nb)
+        self.V = torch.empty(vshape, dtype=wide, device=self.psit.device)
         self.pool = _graph_pool()
         # capture on a side stream with capture_begin/capture_end (the
         # torch.cuda.graph context manager would also run gc.collect() and
@@ -747,7 +817,7 @@ class _GraphedIteration:
     def replay(self):
         self.gA.replay()
         eps, V = torch.linalg.eigh(self.H)
-        self.eps.copy_(eps)
+        self.eps.copy_(eps.reshape(-1))
         self.V.copy_(V)
         self.gB.replay()
         return self.out

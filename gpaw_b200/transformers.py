@@ -90,6 +90,13 @@ class _Transformer:
         if input.dtype.is_complex and phases is None:
             phases = np.ones((3, 2), complex)
         nin = int(np.prod(input.shape[:-3], dtype=np.int64))
+        if input.dtype.is_complex and nat.is_phase_batch(phases):
+            # a k-point batch: nk equal groups of grids, phases[k] each
+            nk, ph = nat.phase_sets(phases)
+            nat.check(nat.lib().gb_transformer_apply_k(
+                self._handle, nat.ptr(input), nat.ptr(output), nin, nat.dtype_code(input),
+                nk, ph, nat.stream_of(input)), 'gb_transformer_apply_k')
+            return output
         nat.check(nat.lib().gb_transformer_apply(
             self._handle, nat.ptr(input), nat.ptr(output), nin,
             nat.dtype_code(input),

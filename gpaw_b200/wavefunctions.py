@@ -28,12 +28,22 @@ def gemm_precision():
 
 
 class KPoint:
-    def __init__(self, psit_nG, q=-1, phase_cd=None, weight=1.0, k_c=None):
+    """The wave functions of one k-point, or of a batch of nk k-points.
+
+    A batch holds nk equal groups of bands in one array (rows k * nbands ..
+    (k + 1) * nbands - 1 belong to k-point k), q = range(nk), phase_cd the
+    (nk, 3, 2) Bloch phases and weight the k-point weight of every row, so
+    that each stencil, preconditioner and LFC launch covers every (k, band);
+    the band-space products are batched over k.  f_n includes the k-point
+    weight (occupation x weight, as the reference's kpt.f_n)."""
+
+    def __init__(self, psit_nG, q=-1, phase_cd=None, weight=1.0, k_c=None, nk=1):
         self.psit_nG = psit_nG
         self.q = q
         self.phase_cd = phase_cd
         self.weight = weight
         self.k_c = np.zeros(3) if k_c is None else np.asarray(k_c, float)
+        self.nk = nk
         self.eps_n = None     # FP64 device tensor after the first subspace step
         self.f_n = None
         self.P_nM = None      # projections <p^a_i|psi_n>, concatenated over atoms
@@ -74,11 +84,17 @@ class FDWaveFunctions:
     def join_M(self, c_axi, xshape):
         return self.pt._gather(c_axi, xshape, self.dtype, self.gd.device)
 
-    def matrix(self, a_nG, b_nG):
-        """dv a^H b as an (n, m) FP64 matrix (one GEMM).  The overlap and
+    def matrix(self, a_nG, b_nG, nk=1):
+        """dv a^H b as an (n, m) FP64 matrix (one GEMM), or (nk, n/nk, m/nk)
+        for a k-point batch (one batched GEMM).  The overlap and
         subspace-Hamiltonian matrices feed Cholesky and eigh, which stay FP64,
         so their sums over grid points are accumulated in FP64 even when
         the wave functions are FP32 (the operands are widened on the fly)."""
+        if nk > 1:
+            wide = torch.complex128 if self.dtype.is_complex else torch.float64
+            A = a_nG.reshape(nk, a_nG.shape[0] // nk, -1).to(wide)
+            B = b_nG.reshape(nk, b_nG.shape[0] // nk, -1).to(wide)
+            return torch.bmm(A.conj(), B.transpose(1, 2)) * self.gd.dv
         if a_nG.dtype == torch.float32 and b_nG.dtype == torch.float32:
             # FP32 real: tensor-core Gram (three-product TF32 split), the
             # diagonal from FP64-accumulated dots
@@ -97,6 +113,21 @@ class FDWaveFunctions:
         becomes kpt.psit_nG -- a captured SCF step writes into its static
         buffer this way instead of copying."""
         psit = kpt.psit_nG
+        nk = getattr(kpt, 'nk', 1)
+        if nk > 1:
+            # per k-point: S_k = L_k L_k^H, psi_k <- L_k^-1 psi_k (batched)
+            S = self.matrix(psit, psit, nk)
+            S = 0.5 * (S + S.conj().transpose(1, 2))
+            L = torch.linalg.cholesky_ex(S)[0]
+            eye = torch.eye(L.shape[-1], dtype=L.dtype, device=L.device).expand_as(L)
+            Linv = torch.linalg.solve_triangular(L, eye, upper=False)
+            C = Linv.conj().to(self.dtype)
+            y = torch.bmm(C, psit.reshape(nk, psit.shape[0] // nk, -1)).reshape(psit.shape)
+            if out is not None:
+                y = out.copy_(y)
+            kpt.psit_nG = y
+            kpt.P_nM = self.projections(kpt.psit_nG, kpt)
+            return
         S = self.matrix(psit, psit).to(torch.complex128 if self.dtype.is_complex
                                          else torch.float64)
         S = 0.5 * (S + S.conj().T)

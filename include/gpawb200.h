@@ -83,6 +83,17 @@ int gb_operator_apply_potential(const gb_operator* op, const void* in,
                                 void* stream);
 /* Weighted-Jacobi relaxation sweeps (relax_method 2) used by the FD Poisson
  * solver: c/operators.c:55-97, c/bmgs/relax.c:7-66.  Real FP64 only. */
+/* A batch of nk k-points in one launch: the nin grids are nk equal groups of
+ * bands (k-point major), group k taking the Bloch phases
+ * phase_kcd[k * 12 .. k * 12 + 11] (the (3, 2) complex phase_cd of that
+ * k-point, re/im interleaved); vt (optional, NULL for none) adds the local
+ * potential as gb_operator_apply_potential does.  nk <= 8.  This is the
+ * loop over kpt_u of gpaw/eigensolvers/eigensolver.py:136-144 folded into
+ * the launch; it has no single counterpart in the reference. */
+int gb_operator_apply_k(const gb_operator* op, const void* in, void* out,
+                        int64_t nin, int dtype, int nk,
+                        const double* phase_kcd, const void* vt, void* stream);
+
 int gb_operator_relax(const gb_operator* op, int relax_method, double* f_g,
                       const double* s_g, int nrelax, double w, void* stream);
 int gb_operator_get_diagonal_element(const gb_operator* op, double* d);
@@ -121,6 +132,10 @@ int gb_transformer_apply_axpy(const gb_transformer* t, const void* in,
                               void* out, int64_t nin, int dtype,
                               const double* phase_cd, double alpha,
                               const void* y, double gamma, void* stream);
+/* nk k-point groups of bands in one launch, phases as gb_operator_apply_k */
+int gb_transformer_apply_k(const gb_transformer* t, const void* in, void* out,
+                           int64_t nin, int dtype, int nk,
+                           const double* phase_kcd, void* stream);
 int gb_transformer_free(gb_transformer* t);
 
 /* ======================================================================
@@ -139,6 +154,17 @@ int gb_fd_precond(const gb_transformer* rest0, const gb_transformer* rest1,
                   const void* residuals, const void* nresiduals,
                   double step, int64_t nin, int dtype,
                   const double* phase_cd, void* stream);
+
+/* The V-cycle for nk k-point groups of bands in one chain of launches,
+ * phases as gb_operator_apply_k (work arrays sized for all nin grids). */
+int gb_fd_precond_k(const gb_transformer* rest0, const gb_transformer* rest1,
+                    const gb_transformer* intp1, const gb_transformer* intp2,
+                    const gb_operator* kin0, const gb_operator* kin1,
+                    const gb_operator* kin2,
+                    void* d0, void* q0, void* r1, void* d1, void* q1,
+                    void* r2, void* d2, void* q2,
+                    const void* residuals, double step, int64_t nin,
+                    int dtype, int nk, const double* phase_kcd, void* stream);
 
 /* The same V-cycle for callers that cannot allocate device memory while
  * they run: a C or Fortran host program that owns only the residual and
@@ -219,6 +245,14 @@ int gb_lfc_add(const gb_lfc* lfc, const void* c_xM, void* a_xG, int64_t nx,
 int gb_lfc_integrate(const gb_lfc* lfc, const void* a_xG, void* c_xM,
                      int64_t nx, int dtype, int q, void* stream);
 int gb_lfc_free(gb_lfc* lfc);
+/* add / integrate over nk k-point groups of the nx rows in one launch:
+ * row x takes the Bloch phases of k-point q = x / (nx / nk) (complex
+ * dtypes; nk <= nq). */
+int gb_lfc_add_k(const gb_lfc* lfc, const void* c_xM, void* a_xG, int64_t nx,
+                 int dtype, int nk, void* stream);
+int gb_lfc_integrate_k(const gb_lfc* lfc, const void* a_xG, void* c_xM,
+                       int64_t nx, int dtype, int nk, void* stream);
+
 /* LFC.derivative (c/lfc.c:1449-1601, called from gpaw/lfc.py:680-682):
  *   c_xMv[x][M][v] += dv sum_G a_xG[x][G] phase_qW d/dr_v Phi_M(r_G - R_W)
  * computed on the fly from the radial splines; arguments as the
