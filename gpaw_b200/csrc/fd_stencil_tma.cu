@@ -24,6 +24,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <cudaTypedefs.h>
 #include "internal.cuh"
 #include "tma.cuh"
@@ -148,7 +149,26 @@ __device__ __forceinline__ void ldg_run(const V* __restrict__ p, V (&v)[N]) {
   }
 }
 
-template <typename T, int H, int R1, int R2, int VB>
+// FP32 taps on two neighbouring points at once (packed f32x2 arithmetic,
+// sm_100): one pair of offsets +k / -k with coefficients cp / cm.  SYM = 1
+// (cp == cm, the Laplacian): c ((vp + vm) - 2 xc), 3 packed operations and
+// exactly zero on a constant; SYM = -1 (cp == -cm, first derivatives):
+// c (vp - vm); SYM = 0: the difference form c (v - xc) per offset.
+template <int SYM>
+__device__ __forceinline__ float2 tap2(float2 acc, float cp, float cm, float2 vp, float2 vm, float2 xc) {
+  const float2 m1 = make_float2(-1.f, -1.f);
+  if constexpr (SYM == 1) {
+    const float2 d = __ffma2_rn(make_float2(-2.f, -2.f), xc, __fadd2_rn(vp, vm));
+    return __ffma2_rn(make_float2(cp, cp), d, acc);
+  } else if constexpr (SYM == -1) {
+    return __ffma2_rn(make_float2(cp, cp), __ffma2_rn(vm, m1, vp), acc);
+  } else {
+    acc = __ffma2_rn(make_float2(cp, cp), __ffma2_rn(xc, m1, vp), acc);
+    return __ffma2_rn(make_float2(cm, cm), __ffma2_rn(xc, m1, vm), acc);
+  }
+}
+
+template <typename T, int H, int R1, int R2, int VB, int SYM = 0>
 __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                         const __grid_constant__ CUtensorMap tmH,
                                                         const __grid_constant__ CUtensorMap tmB,
@@ -265,6 +285,7 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
   // operator exactly constant-annihilating after the coefficients are rounded
   // (otherwise every eigenvalue shifts by ~|c0| 2^-24)
   constexpr bool DIFF = sizeof(R) == 4;
+  constexpr bool PACK = std::is_same<T, float>::value && R2 % 2 == 0;
   const bool epi = a.alpha != 1.0 || a.beta != 0.0 || a.y != nullptr || a.vpot != nullptr;
   const R* __restrict__ vpot = reinterpret_cast<const R*>(a.vpot);
 
@@ -305,6 +326,85 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
           const int cpl = p_start + t - 2 * H;
           const unsigned char* Pc = slots + (int64_t)cslot * a.slot_bytes;
           T acc[R1][R2];
+          if constexpr (PACK) {
+          // FP32: two points per instruction (f32x2), pairs of columns
+          float2 acc2[R1][R2 / 2];
+          // centre + axis 0 (register queue)
+#pragma unroll
+          for (int r = 0; r < R1; ++r)
+#pragma unroll
+            for (int p = 0; p < R2 / 2; ++p) {
+              const float2 xc = make_float2(q[cu][r][2 * p], q[cu][r][2 * p + 1]);
+              float2 x = __fmul2_rn(make_float2(a.c0difff, a.c0difff), xc);
+#pragma unroll
+              for (int k = 1; k <= H; ++k) {
+                const int mp = (u + 1 + H + k) % NQ, mm = (u + 1 + H - k) % NQ;
+                x = tap2<SYM>(x, coef<R>(a, 0, HMAX + k), coef<R>(a, 0, HMAX - k),
+                              make_float2(q[mp][r][2 * p], q[mp][r][2 * p + 1]),
+                              make_float2(q[mm][r][2 * p], q[mm][r][2 * p + 1]), xc);
+              }
+              acc2[r][p] = x;
+            }
+          // axis 2: the row with its halo chunks
+#pragma unroll
+          for (int r = 0; r < R1; ++r) {
+            float w[HZ + R2 + HZ];
+#pragma unroll
+            for (int ch = 0; ch < HZ / VEC; ++ch) {
+              T tl[VEC], tr[VEC];
+              ldv<T, VEC, VB>(reinterpret_cast<const T*>(Pc + lcol[ch] + r * pitch), tl);
+              ldv<T, VEC, VB>(reinterpret_cast<const T*>(Pc + rcol[ch] + r * pitch), tr);
+#pragma unroll
+              for (int v = 0; v < VEC; ++v) {
+                w[ch * VEC + v] = tl[v];
+                w[HZ + R2 + ch * VEC + v] = tr[v];
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < R2; ++c) w[HZ + c] = q[cu][r][c];
+#pragma unroll
+            for (int p = 0; p < R2 / 2; ++p) {
+              const int c = HZ + 2 * p;
+              const float2 xc = make_float2(w[c], w[c + 1]);
+              float2 x = acc2[r][p];
+#pragma unroll
+              for (int k = 1; k <= H; ++k)
+                x = tap2<SYM>(x, coef<R>(a, 2, HMAX + k), coef<R>(a, 2, HMAX - k),
+                              make_float2(w[c + k], w[c + 1 + k]), make_float2(w[c - k], w[c + 1 - k]), xc);
+              acc2[r][p] = x;
+            }
+          }
+          // axis 1: rows of the centre slot, streamed (difference form)
+#pragma unroll
+          for (int rr = -H; rr < R1 + H; ++rr) {
+            T v[R2];
+            if (rr >= 0 && rr < R1) {
+#pragma unroll
+              for (int c = 0; c < R2; ++c) v[c] = q[cu][rr][c];
+            } else {
+              ldv<T, R2, VB>(reinterpret_cast<const T*>(Pc + own_row + rr * pitch + own_col), v);
+            }
+#pragma unroll
+            for (int r = 0; r < R1; ++r) {
+              const int d = rr - r;
+              if (d < -H || d > H || d == 0) continue;
+              const float cc = coef<R>(a, 1, HMAX + d);
+#pragma unroll
+              for (int p = 0; p < R2 / 2; ++p) {
+                const float2 xc = make_float2(q[cu][r][2 * p], q[cu][r][2 * p + 1]);
+                const float2 dv = __ffma2_rn(xc, make_float2(-1.f, -1.f), make_float2(v[2 * p], v[2 * p + 1]));
+                acc2[r][p] = __ffma2_rn(make_float2(cc, cc), dv, acc2[r][p]);
+              }
+            }
+          }
+#pragma unroll
+          for (int r = 0; r < R1; ++r)
+#pragma unroll
+            for (int p = 0; p < R2 / 2; ++p) {
+              acc[r][2 * p] = acc2[r][p].x;
+              acc[r][2 * p + 1] = acc2[r][p].y;
+            }
+          } else {
           // centre + axis 0 (register queue)
 #pragma unroll
           for (int r = 0; r < R1; ++r)
@@ -366,6 +466,7 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
                 acc[r][c] = fmadd(acc[r][c], coef<R>(a, 1, m + HMAX - H), DIFF ? sub(v[c], q[cu][r][c]) : v[c]);
             }
           }
+          }  // PACK
           // epilogue + streaming stores
           if (active) {
             const int64_t pbase = (int64_t)cpl * n12 + (int64_t)yrow * n2 + tz * R2;
@@ -383,12 +484,27 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
                   R vv[R2];
                   if (ybase) ldg_run<T, R2>(ybase + p, yv);
                   if (vpot) ldg_run<R, R2>(vpot + p, vv);
+                  if constexpr (PACK) {
+                    const float2 al = make_float2((float)a.alpha, (float)a.alpha);
+                    const float2 be = make_float2((float)a.beta, (float)a.beta);
+                    const float2 ga = make_float2((float)a.gamma, (float)a.gamma);
+#pragma unroll
+                    for (int c = 0; c < R2; c += 2) {
+                      const float2 xc = make_float2(q[cu][r][c], q[cu][r][c + 1]);
+                      float2 v = __ffma2_rn(be, xc, __fmul2_rn(al, make_float2(acc[r][c], acc[r][c + 1])));
+                      if (ybase) v = __ffma2_rn(ga, make_float2(yv[c], yv[c + 1]), v);
+                      if (vpot) v = __ffma2_rn(make_float2(vv[c], vv[c + 1]), xc, v);
+                      acc[r][c] = v.x;
+                      acc[r][c + 1] = v.y;
+                    }
+                  } else {
 #pragma unroll
                   for (int c = 0; c < R2; ++c) {
                     T v = fmadd(scale((R)a.alpha, acc[r][c]), (R)a.beta, q[cu][r][c]);
                     if (ybase) v = fmadd(v, (R)a.gamma, yv[c]);
                     if (vpot) v = fmadd(v, vv[c], q[cu][r][c]);
                     acc[r][c] = v;
+                  }
                   }
                 } else {
 #pragma unroll
@@ -442,13 +558,13 @@ __global__ void __launch_bounds__(512) star_tma_kernel(const __grid_constant__ C
 }
 
 // ------------------------------------------------------------------ host
-template <typename T, int H, int R1, int R2, int VB = 16>
+template <typename T, int H, int R1, int R2, int VB = 16, int SYM = 0>
 static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int64_t nin, cudaStream_t st,
                           const Epilogue& ep) {
   using R = typename Elem<T>::R;
   const int n0 = (int)op->n[0], n1 = (int)op->n[1], n2 = (int)op->n[2];
   const int TZ = n2 / R2;
-  auto kern = star_tma_kernel<T, H, R1, R2, VB>;
+  auto kern = star_tma_kernel<T, H, R1, R2, VB, SYM>;
   static int regs = -1;
   if (regs < 0) {
     cudaFuncAttributes fa;
@@ -582,8 +698,8 @@ static int launch_tma_cfg(const gb_operator* op, const void* in, void* out, int6
   // fails, the model's best candidate is used without tuning.
   const int epi_kind = (ep.vpot ? 4 : 0) | (ep.y ? 2 : 0) | ((ep.alpha != 1.0 || ep.beta != 0.0) ? 1 : 0);
   char keyb[160];
-  snprintf(keyb, sizeof keyb, "%d:%d:%d:%d:%d:%d:%d:%d:%d:%d:%lld", (int)sizeof(T), Elem<T>::cplx ? 1 : 0, H, n0, n1,
-           n2, op->pbc[0] * 4 + op->pbc[1] * 2 + op->pbc[2], epi_kind, (int)VB, R2, (long long)nin);
+  snprintf(keyb, sizeof keyb, "%d:%d:%d:%d:%d:%d:%d:%d:%d:%d:%d:%lld", (int)sizeof(T), Elem<T>::cplx ? 1 : 0, H, n0,
+           n1, n2, op->pbc[0] * 4 + op->pbc[1] * 2 + op->pbc[2], epi_kind, (int)VB, R2, SYM, (long long)nin);
   const std::string key(keyb);
   int choice = -1;
   {
@@ -670,13 +786,30 @@ int star_tma_apply(const gb_operator* op, const void* in, void* out, int64_t nin
         case 3: return launch_tma_cfg<double, 3, 2, 2>(op, in, out, nin, st, ep);
         default: return launch_tma_cfg<double, 4, 2, 2>(op, in, out, nin, st, ep);
       }
-    case GB_DTYPE_F32:
+    case GB_DTYPE_F32: {
+      // coefficient symmetry of every axis, in FP32: symmetric pairs (the
+      // Laplacian) and antisymmetric pairs (derivatives) take fewer
+      // operations in the packed kernel
+      bool sym = true, anti = true;
+      for (int c = 0; c < 3; ++c)
+        for (int k = 1; k <= HMAX; ++k) {
+          const float p = (float)op->a[c][HMAX + k], m = (float)op->a[c][HMAX - k];
+          sym = sym && p == m;
+          anti = anti && p == -m;
+        }
+      const int kind = sym ? 1 : (anti ? -1 : 0);
+#define GB_F32_TMA(HH)                                                                      \
+  return kind == 1 ? launch_tma_cfg<float, HH, 2, 4, 16, 1>(op, in, out, nin, st, ep)       \
+                   : kind == -1 ? launch_tma_cfg<float, HH, 2, 4, 16, -1>(op, in, out, nin, st, ep) \
+                                : launch_tma_cfg<float, HH, 2, 4, 16, 0>(op, in, out, nin, st, ep)
       switch (op->H) {
-        case 1: return launch_tma_cfg<float, 1, 2, 4>(op, in, out, nin, st, ep);
-        case 2: return launch_tma_cfg<float, 2, 2, 4>(op, in, out, nin, st, ep);
-        case 3: return launch_tma_cfg<float, 3, 2, 4>(op, in, out, nin, st, ep);
-        default: return launch_tma_cfg<float, 4, 2, 4>(op, in, out, nin, st, ep);
+        case 1: GB_F32_TMA(1);
+        case 2: GB_F32_TMA(2);
+        case 3: GB_F32_TMA(3);
+        default: GB_F32_TMA(4);
       }
+#undef GB_F32_TMA
+    }
     case GB_DTYPE_C128:
       switch (op->H) {
         case 1: return launch_tma_cfg<double2, 1, 2, 1>(op, in, out, nin, st, ep);

@@ -512,8 +512,8 @@ class Calculation:
           ion charges    -(derivative of int v_H rhot through the Gaussian
                          ion charge -Z g/I(R), normalised on the grid)
           ion-ion        the geometry constant's gradient
-        Device work in the precision of the run (sums in FP64); the small
-        per-atom reductions on the host."""
+        Evaluated in FP64 (an FP32 run's wave functions are widened first);
+        the small per-atom reductions on the host."""
         natoms = len(self.setups)
         F = np.zeros((natoms, 3))
         pt = self.wfs.pt
@@ -527,8 +527,12 @@ class Calculation:
                 for k in range(nk):
                     rows = slice(k * nb, (k + 1) * nb)
                     q = (k if nk > 1 else kpt.q) if self.dtype.is_complex else -1
-                    D = pt.derivative(kpt.psit_nG[rows].contiguous(), {}, q).to(wide)
-                    C = kpt.P_nM[rows].to(wide) @ self.dH_MM.to(wide).T
+                    # projections and their derivatives from the state widened
+                    # to FP64 (FP32 runs: the force sums stay FP64, like the
+                    # energy sums)
+                    psi = kpt.psit_nG[rows].to(wide).contiguous()
+                    D = pt.derivative(psi, {}, q)
+                    C = pt.integrate(psi, {}, q) @ self.dH_MM.to(wide).T
                     # 2 Re sum_n f_n conj(D_nMv) C_nM
                     F_Mv += 2 * (f_n[rows, None, None] * (D.conj() * C[:, :, None]).real).sum(0)
             F_Mv = F_Mv.cpu().numpy()
