@@ -63,6 +63,7 @@ _SIGNATURES = {
     'gb_lfc_integrate': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int,
                                  c_int, c_void_p]),
     'gb_lfc_free': (c_int, [c_void_p]),
+    'gb_lfc_tiled': (c_int, [c_void_p]),
     'gb_add_to_density': (c_int, [c_int64, c_void_p, c_void_p, c_int, c_int64,
                                   c_void_p, c_void_p]),
     'gb_conv3d_forward': (c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int,

@@ -167,61 +167,97 @@ __global__ void __launch_bounds__(256, CC > 1 ? 2 : 3) fold_fine_kernel(const Fo
 }
 
 // Level 0 (rh = 1, one coarse channel), marching along axis 0.  A CTA owns
-// TY full rows (j0 .. j0 + TY - 1) of one band over a chunk of planes; each
-// input plane p is staged once (cp.async, rows j0 - 1 .. j0 + TY with the
-// periodic halo columns) and every thread turns it into the three partial
-// sums S_dx(p) = sum_{dy,dz} W0[dx][dy][dz] x[p][j + dy][k + dz] of its 4
-// points, added to the output planes p - 1, p, p + 1 held in a register
-// queue: 4.5 shared loads and 27 FMAs per point for the fine part.  When
-// output plane o = p - 1 is complete, the coarse part
-// sum_e H[(o%2) - 2ex][..][..] b1[o/2 + e] is added from staged coarse
-// planes (a ring of 4; zero taps of the parity skipped) and the 4 points
-// are stored as one 16-byte vector.  Requires n2 % 4 == 0, periodic axes.
-template <int TY>
-__global__ void __launch_bounds__(256) fold0_march_kernel(const FoldArgs a, int nch) {
-  __shared__ float sW[27];
-  __shared__ float sH[216];
+// TY full rows j0 .. j0 + TY - 1 (TY even, n1 % TY == 0) of one band over a
+// chunk of planes; a thread owns the 4 points k .. k + 3 of an even row j
+// and of the odd row j + 1 (8 outputs).  Each input plane p is staged once
+// (cp.async into a ring of three slots: the copy of plane p + 2 is issued
+// right after the single barrier of the step) and every thread adds
+// W0[dx][dy][dz] x[p][.][.] over its four input rows j - 1 .. j + 2 to the
+// output planes p + 1 - dx held in a register queue -- 12 shared loads and
+// 216 FMAs per plane, the 27 weights in registers.  When output plane
+// o = p - 1 is complete, the coarse part
+// sum_e H[(o%2) - 2ex][(j%2) - 2ey][..] b1[o/2 + e] is added from staged
+// coarse planes (a ring of 4; zero taps of the parities skipped; both rows
+// read the same three coarse rows) and the 8 points are stored as two
+// 16-byte vectors.  Row pitches FP, CP (floats) are chosen on the host so
+// that the lanes of a quarter warp (fine, 16-byte loads) or half warp
+// (coarse, 8-byte loads) hit distinct banks.  Requires n2 % 4 == 0 and
+// periodic axes.
+struct Fold0Cfg {
+  int TY, FP, CP, nch;
+};
+
+__global__ void __launch_bounds__(512) fold0_pair_kernel(const FoldArgs a, const Fold0Cfg cfg) {
+  __shared__ __align__(16) float sH[36 * 8];           // [tx][ty][tz 0..7]: H, tz >= 6 zero
   extern __shared__ __align__(16) float fm_smem[];
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2;
   const int m0 = n0 >> 1, m1 = n1 >> 1, m2 = n2 >> 1;
-  const int FP = n2 + 8, CP = m2 + 8;                 // staged row pitches (column c at 4 + c)
-  constexpr int FR = TY + 2, CR = TY / 2 + 2;
-  float* fslot = fm_smem;                             // [2][FR][FP]
-  float* cslot = fm_smem + 2 * FR * FP;               // [4][CR][CP]
+  const int TY = cfg.TY, FP = cfg.FP, CP = cfg.CP;    // fine column c at 4 + c, coarse at 5 + c
+  const int FR = TY + 2, CR = TY / 2 + 2;
+  float* fslot = fm_smem;                              // [3][FR][FP]
+  float* cslot = fm_smem + 3 * FR * FP;                // [4][CR][CP]
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int e = tid; e < 27; e += nt) sW[e] = a.F[e];
-  for (int e = tid; e < 216; e += nt) sH[e] = a.G[e];
+  for (int e = tid; e < 36 * 8; e += nt) sH[e] = (e & 7) < 6 ? a.G[(e >> 3) * 6 + (e & 7)] : 0.f;
+  float W[27];
+#pragma unroll
+  for (int e = 0; e < 27; ++e) W[e] = __ldg(a.F + e);
   const int ngx = n2 >> 2;
-  const int gx = tid % ngx, ty = tid / ngx;
+  const int gx = tid % ngx, rp = tid / ngx;
   const int j0 = blockIdx.y * TY;
-  const int j = j0 + ty, k = 4 * gx;
+  const int j = j0 + 2 * rp, k = 4 * gx;
   const int64_t b = blockIdx.z;
-  const int o_beg = (int)((int64_t)blockIdx.x * n0 / nch), o_end = (int)((int64_t)(blockIdx.x + 1) * n0 / nch);
+  const int o_beg = (int)((int64_t)blockIdx.x * n0 / cfg.nch), o_end = (int)((int64_t)(blockIdx.x + 1) * n0 / cfg.nch);
   const float* xb = a.xf + b * n0 * (int64_t)n1 * n2;
   const float* cb = a.xc + b * (int64_t)m0 * m1 * m2;
 
-  // staging: thread (ty, gx) copies rows ty, ty + TY, ... and 16-byte
-  // chunks gx, gx + ngx, ... (no index divisions); the two halo columns of
-  // a row come from the threads gx = 0 and 1
+  // the (row, 16-byte chunk) pieces of a staged plane this thread copies:
+  // pieces tid, tid + nt, ... (at most 4 per thread), offsets fixed per CTA
+  int f_src[4], f_dst[4];
+  int nf = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int e = tid + u * nt;
+    f_src[u] = 0;
+    f_dst[u] = 0;
+    if (e < FR * ngx) {
+      const int r = e / ngx, c = e % ngx;
+      f_src[u] = pw(j0 - 1 + r, n1) * n2 + 4 * c;
+      f_dst[u] = r * FP + 4 + 4 * c;
+      nf = u + 1;
+    }
+  }
   auto stage_fine = [&](int p, float* dst) {
     const float* pl = xb + (int64_t)pw(p, n0) * n1 * n2;
-    for (int r = ty; r < FR; r += TY) {
-      const float* row = pl + (int64_t)pw(j0 - 1 + r, n1) * n2;
-      float* d = dst + r * FP;
-      for (int c = gx; c < ngx; c += ngx) cp_async16(d + 4 + 4 * c, row + 4 * c);
-      if (gx == 0) cp_async4(d + 3, row + n2 - 1);                 // column -1
-      if (gx == 1 || ngx == 1) cp_async4(d + 4 + n2, row);         // column n2
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (u < nf) cp_async16(dst + f_dst[u], pl + f_src[u]);
+    // the two periodic halo columns of every row
+    for (int e = tid; e < 2 * FR; e += nt) {
+      const int r = e >> 1, row = pw(j0 - 1 + r, n1) * n2;
+      if (e & 1) cp_async4(dst + r * FP + 4 + n2, pl + row);       // column n2
+      else cp_async4(dst + r * FP + 3, pl + row + n2 - 1);         // column -1
     }
   };
+  // the coarse elements (row r, column c = -1 .. m2) this thread copies
+  int c_src[4], c_dst[4];
+  int ncp = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int e = tid + u * nt;
+    c_src[u] = 0;
+    c_dst[u] = 0;
+    if (e < CR * (m2 + 2)) {
+      const int r = e / (m2 + 2), c = e % (m2 + 2) - 1;
+      c_src[u] = pw((j0 >> 1) - 1 + r, m1) * m2 + pw(c, m2);
+      c_dst[u] = r * CP + 5 + c;
+      ncp = u + 1;
+    }
+  }
   auto stage_coarse = [&](int C, float* dst) {
     const float* pl = cb + (int64_t)pw(C, m0) * m1 * m2;
-    for (int r = ty; r < CR; r += TY) {
-      const float* row = pl + (int64_t)pw((j0 >> 1) - 1 + r, m1) * m2;
-      float* d = dst + r * CP;
-      for (int c = gx; c < (m2 >> 1); c += ngx) cp_async8(d + 4 + 2 * c, row + 2 * c);
-      if (gx == 0) cp_async4(d + 3, row + m2 - 1);
-      if (gx == 1 || ngx == 1) cp_async4(d + 4 + m2, row);
-    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (u < ncp) cp_async4(dst + c_dst[u], pl + c_src[u]);
   };
   auto cidx = [](int C) { return (C + 4) & 3; };
 
@@ -233,85 +269,23 @@ __global__ void __launch_bounds__(256) fold0_march_kernel(const FoldArgs a, int 
   stage_fine(o_beg, fslot + FR * FP);
   cp_async_commit();
 
-  float qa[4] = {0.f, 0.f, 0.f, 0.f}, qb[4] = {0.f, 0.f, 0.f, 0.f}, qc[4] = {0.f, 0.f, 0.f, 0.f};
-  const bool act = ty < TY && j < n1;
-  __syncthreads();                                  // sW, sH written
+  // output planes p - 1, p, p + 1 (rows j, j + 1) of the step with input p
+  float qa[2][4], qb[2][4], qc[2][4];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) qa[r][q] = qb[r][q] = qc[r][q] = 0.f;
+  const bool act = rp < TY / 2;
 
   const int nsteps = o_end - o_beg + 2;
   for (int st = 0; st < nsteps; ++st) {
     const int p = o_beg - 1 + st;
     cp_async_wait<1>();
     __syncthreads();
-    if (act) {
-      const float* F = fslot + (st & 1) * FR * FP;
-      float S[3][4];
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) S[d][q] = 0.f;
-#pragma unroll
-      for (int dy = 0; dy < 3; ++dy) {
-        // three 16-byte loads (scalar neighbours at a 4-float thread
-        // stride would be 4-way bank conflicts)
-        const float* rp = F + (ty + dy) * FP + 4 + k;
-        const float4 l4 = *reinterpret_cast<const float4*>(rp - 4);
-        const float4 m4 = *reinterpret_cast<const float4*>(rp);
-        const float4 r4 = *reinterpret_cast<const float4*>(rp + 4);
-        const float v[6] = {l4.w, m4.x, m4.y, m4.z, m4.w, r4.x};
-#pragma unroll
-        for (int dx = 0; dx < 3; ++dx)
-#pragma unroll
-          for (int dz = 0; dz < 3; ++dz) {
-            const float w = sW[dx * 9 + dy * 3 + dz];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) S[dx][q] = fmaf(w, v[q + dz], S[dx][q]);
-          }
-      }
-      // plane p is x[o + dx] for o = p - dx: dx = +1 -> o = p - 1, ...
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        qa[q] += S[2][q];
-        qb[q] += S[1][q];
-        qc[q] += S[0][q];
-      }
-      const int o = p - 1;
-      if (o >= o_beg) {
-        // coarse part of output plane o
-        const int px = o & 1, I0 = o >> 1, py = j & 1, K0 = k >> 1;
-#pragma unroll
-        for (int ex = -1; ex <= 1; ++ex) {
-          const int tx = px - 2 * ex + 2;
-          if (tx > 4) continue;
-          const float* Cs = cslot + cidx(I0 + ex) * CR * CP;
-#pragma unroll
-          for (int ey = -1; ey <= 1; ++ey) {
-            const int tyy = py - 2 * ey + 2;
-            if (tyy > 4) continue;
-            const float* cr = Cs + ((ty >> 1) + 1 + ey) * CP + 3 + K0;
-            const float c0 = cr[0], c1 = cr[1], c2 = cr[2], c3 = cr[3];
-            const float* g = sH + (tx * 6 + tyy) * 6;
-            const float g0 = g[0], g1 = g[1], g2 = g[2], g3 = g[3], g4 = g[4];
-            qa[0] = fmaf(g4, c0, fmaf(g2, c1, fmaf(g0, c2, qa[0])));
-            qa[1] = fmaf(g3, c1, fmaf(g1, c2, qa[1]));
-            qa[2] = fmaf(g4, c1, fmaf(g2, c2, fmaf(g0, c3, qa[2])));
-            qa[3] = fmaf(g3, c2, fmaf(g1, c3, qa[3]));
-          }
-        }
-        float* yp = a.y + ((b * n0 + o) * (int64_t)n1 + j) * n2 + k;
-        *reinterpret_cast<float4*>(yp) = make_float4(qa[0], qa[1], qa[2], qa[3]);
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        qa[q] = qb[q];
-        qb[q] = qc[q];
-        qc[q] = 0.f;
-      }
-    }
-    __syncthreads();
-    // refill: fine plane p + 2 into this step's slot, and the coarse plane
-    // the output completed two steps later needs
+    // refill: fine plane p + 2 into the slot step st - 1 used, and the coarse
+    // plane the output completed two steps later needs
     if (p + 2 <= o_end) {
-      stage_fine(p + 2, fslot + (st & 1) * FR * FP);
+      stage_fine(p + 2, fslot + ((st + 2) % 3) * FR * FP);
       const int Cn = ((p + 1) >> 1) + 1;
       if (Cn > c_last) {
         stage_coarse(Cn, cslot + cidx(Cn) * CR * CP);
@@ -319,8 +293,91 @@ __global__ void __launch_bounds__(256) fold0_march_kernel(const FoldArgs a, int 
       }
     }
     cp_async_commit();
+    if (act) {
+      const float* F = fslot + (st % 3) * FR * FP;
+#pragma unroll
+      for (int R = 0; R < 4; ++R) {
+        // input row j - 1 + R: dy = R for row j, R - 1 for row j + 1
+        const float* rpp = F + (2 * rp + R) * FP + 4 + k;
+        const float4 l4 = *reinterpret_cast<const float4*>(rpp - 4);
+        const float4 m4 = *reinterpret_cast<const float4*>(rpp);
+        const float4 r4 = *reinterpret_cast<const float4*>(rpp + 4);
+        const float v[6] = {l4.w, m4.x, m4.y, m4.z, m4.w, r4.x};
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+          // plane p is x[o + dx - 1] of output o = p + 1 - dx
+          float(&Q)[2][4] = dx == 2 ? qa : (dx == 1 ? qb : qc);
+#pragma unroll
+          for (int dz = 0; dz < 3; ++dz) {
+            if (R <= 2) {
+              const float w = W[dx * 9 + R * 3 + dz];
+#pragma unroll
+              for (int q = 0; q < 4; ++q) Q[0][q] = fmaf(w, v[q + dz], Q[0][q]);
+            }
+            if (R >= 1) {
+              const float w = W[dx * 9 + (R - 1) * 3 + dz];
+#pragma unroll
+              for (int q = 0; q < 4; ++q) Q[1][q] = fmaf(w, v[q + dz], Q[1][q]);
+            }
+          }
+        }
+      }
+      const int o = p - 1;
+      if (o >= o_beg) {
+        // coarse part of output plane o; coarse row of j and j + 1: j / 2
+        const int px = o & 1, I0 = o >> 1, K0 = k >> 1;
+#pragma unroll
+        for (int ex = -1; ex <= 1; ++ex) {
+          const int tx = px - 2 * ex + 2;
+          if (tx > 4) continue;
+          const float* Cs = cslot + cidx(I0 + ex) * CR * CP;
+          float c[3][4];                                  // coarse rows J - 1 .. J + 1, cols K0 - 1 .. K0 + 2
+#pragma unroll
+          for (int e = 0; e < 3; ++e) {
+            const float* cr = Cs + (rp + e) * CP + 4 + K0;
+            const float2 u = *reinterpret_cast<const float2*>(cr), w = *reinterpret_cast<const float2*>(cr + 2);
+            c[e][0] = u.x; c[e][1] = u.y; c[e][2] = w.x; c[e][3] = w.y;
+          }
+          const float* gt = sH + tx * 48;
+#pragma unroll
+          for (int e = 0; e < 5; ++e) {
+            // e = 0, 1, 2: row j (tyy = 4, 2, 0 for ey = -1, 0, 1); e = 3, 4:
+            // row j + 1 (tyy = 3, 1 for ey = 0, 1)
+            const int r = e < 3 ? 0 : 1;
+            const int ey = e < 3 ? e - 1 : e - 3;
+            const int tyy = e < 3 ? 4 - 2 * e : 3 - 2 * (e - 3);
+            const float4 g03 = *reinterpret_cast<const float4*>(gt + tyy * 8);
+            const float g4 = gt[tyy * 8 + 4];
+            const float* cv = c[ey + 1];
+            qa[r][0] = fmaf(g4, cv[0], fmaf(g03.z, cv[1], fmaf(g03.x, cv[2], qa[r][0])));
+            qa[r][1] = fmaf(g03.w, cv[1], fmaf(g03.y, cv[2], qa[r][1]));
+            qa[r][2] = fmaf(g4, cv[1], fmaf(g03.z, cv[2], fmaf(g03.x, cv[3], qa[r][2])));
+            qa[r][3] = fmaf(g03.w, cv[2], fmaf(g03.y, cv[3], qa[r][3]));
+          }
+        }
+        float* yp = a.y + ((b * n0 + o) * (int64_t)n1 + j) * n2 + k;
+        *reinterpret_cast<float4*>(yp) = make_float4(qa[0][0], qa[0][1], qa[0][2], qa[0][3]);
+        *reinterpret_cast<float4*>(yp + n2) = make_float4(qa[1][0], qa[1][1], qa[1][2], qa[1][3]);
+      }
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          qa[r][q] = qb[r][q];
+          qb[r][q] = qc[r][q];
+          qc[r][q] = 0.f;
+        }
+    }
   }
   cp_async_wait<0>();
+}
+
+// smallest pitch >= lo, a multiple of 4 (16-byte rows), congruent to r
+// modulo m where that is possible (else lo rounded up to 4)
+static int bank_pitch(int lo, int r, int m) {
+  for (int p = (lo + 3) / 4 * 4; p < lo + m + 4; p += 4)
+    if (p % m == r % m) return p;
+  return (lo + 3) / 4 * 4;
 }
 
 // r2[b][c][I] = sum_d Q[d][c] r1[b][2I + d], d in [-2, 2]^3, 16 channels
@@ -550,17 +607,48 @@ int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* x
   FoldArgs a{xf, xc, y, F, G, nb, (int)n_c[0], (int)n_c[1], (int)n_c[2]};
   cudaStream_t st = (cudaStream_t)stream;
   if (rh == 1 && cc == 1) {
+    // a quarter warp spans <= 2 row pairs: consecutive 16-byte chunks when
+    // a row pair advances the chunk index by ngx (mod 8); likewise the
+    // coarse 8-byte loads (mod 16) of a half warp
     const int ngx = (int)(n_c[2] / 4);
-    const int TY = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
-    if (n_c[2] % 4 == 0 && n_c[1] % 2 == 0 && ngx * 2 <= 256 && n_c[1] >= TY + 2 && n_c[0] >= 2) {
-      const int nch = (int)std::min<int64_t>(n_c[0], std::max<int64_t>(1, n_c[0] / 12));
-      const size_t smem = (size_t)(2 * (TY + 2) * (n_c[2] + 8) + 4 * (TY / 2 + 2) * (n_c[2] / 2 + 8)) * sizeof(float);
-      const dim3 grid((unsigned)nch, (unsigned)((n_c[1] + TY - 1) / TY), (unsigned)nb);
-      const unsigned threads = (unsigned)(ngx * TY);
-      if (TY == 8) fold0_march_kernel<8><<<grid, threads, smem, st>>>(a, nch);
-      else if (TY == 4) fold0_march_kernel<4><<<grid, threads, smem, st>>>(a, nch);
-      else fold0_march_kernel<2><<<grid, threads, smem, st>>>(a, nch);
-      return check_launch("fold0_march_kernel");
+    Fold0Cfg cfg;
+    cfg.FP = bank_pitch((int)n_c[2] + 8, (int)(n_c[2] / 2), 16);
+    cfg.CP = bank_pitch((int)(n_c[2] / 2) + 8, (int)(n_c[2] / 2), 32);
+    auto smem_of = [&](int t) {
+      return (size_t)(3 * (t + 2) * cfg.FP + 4 * (t / 2 + 2) * cfg.CP) * sizeof(float);
+    };
+    static size_t attr = 0;
+    if (attr == 0) {
+      cudaFuncSetAttribute(fold0_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      attr = 1;
+    }
+    // rows per CTA: the even divisor of n1 (<= 512 threads of 2 rows x 4
+    // points, plane pieces <= 4 per thread) with the most resident warps
+    // doing work per SM; ties to more rows (less halo)
+    int TY = 0;
+    double best = 0.0;
+    for (int t = (int)n_c[1]; t >= 2; t -= 2) {
+      const int thr = ngx * t / 2;
+      if (n_c[1] % t || thr > 512 || (t + 2) * ngx > 4 * thr || (t / 2 + 2) * (n_c[2] / 2 + 2) > 4 * thr ||
+          smem_of(t) > 200 * 1024)
+        continue;
+      int blk = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blk, fold0_pair_kernel, thr, smem_of(t));
+      const double busy = (double)blk * thr;
+      if (busy > best * 1.001) {
+        best = busy;
+        TY = t;
+      }
+    }
+    if (TY && n_c[2] % 4 == 0 && n_c[0] >= 2) {
+      cfg.TY = TY;
+      const int threads = ngx * TY / 2;
+      const size_t smem = smem_of(TY);
+      // plane chunks of about 12 planes (two halo planes each)
+      cfg.nch = (int)std::max<int64_t>(1, n_c[0] / 12);
+      const dim3 grid((unsigned)cfg.nch, (unsigned)(n_c[1] / TY), (unsigned)nb);
+      fold0_pair_kernel<<<grid, (unsigned)threads, smem, st>>>(a, cfg);
+      return check_launch("fold0_pair_kernel");
     }
     return launch_fine(fold_fine_kernel<1, 1>, a, "fold_fine_kernel<1,1>", st);
   }

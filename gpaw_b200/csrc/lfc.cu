@@ -65,6 +65,32 @@ struct gb_lfc {
   bool full64 = false;        // the same with multiples of 2 (16-byte FP64 loads)
   float* Ac32 = nullptr;      // [C][fast_nmax]
   double* Ac64 = nullptr;
+  // brick-tiled FP32 add / integrate for real data (every volume has <= 8
+  // functions, nG a multiple of 4): 32-point chunks of four 8-point
+  // sub-tiles; one entry per (volume, sub-tile it touches) with the volume's
+  // values there as a dense [m][p] 8 x 8 block (zero where the volume does
+  // not cover the point or m >= nm); bricks of consecutive chunks
+  bool tiled = false;
+  int* tch_c = nullptr;       // [nch] chunk index of every chunk with entries
+  int* tch_eoff = nullptr;    // [4 nch + 1] entries of (chunk, sub-tile)
+  int* te_info = nullptr;     // [ne] slot in its brick | nm << 8
+  float* te_A = nullptr;      // [ne][8][8]
+  int tbr_n = 0;              // bricks
+  int tbr_smax = 1;           // most slots in a brick
+  int tbr_emax = 0;           // most entries in a brick
+  int* tbr_ch0 = nullptr;     // [tbr_n + 1] chunk range of each brick
+  int* tbr_pbase = nullptr;   // [tbr_n + 1] first (brick, slot) pair
+  int64_t tpart_n = 0;        // (brick, slot) pairs
+  int* tps_M = nullptr;       // [tpart_n] their group's first function
+  int* tps_nm = nullptr;      // [tpart_n] and function count
+  int* tps_eoff = nullptr;    // [tpart_n + 1] their entries:
+  int* tps_info = nullptr;    //   (entry - brick's first) | sub-tile << 16 | nm << 24
+  int* tgr_poff = nullptr;    // [ngroups + 1] the (brick, slot) pairs of each
+  int* tgr_pidx = nullptr;    //   group, in brick order
+  // work space of the tiled path (transposed coefficients, partial sums);
+  // grown outside stream capture only
+  mutable void* work = nullptr;
+  mutable size_t work_bytes = 0;
   std::vector<void*> allocations;
 };
 
@@ -520,9 +546,16 @@ static int add_fast(const gb_lfc* l, const void* c, void* a, int64_t nx, cudaStr
   return check_launch("lfc_add_bands_kernel");
 }
 
+static bool tiles_usable(const gb_lfc* l, const void* a);
+static int integrate_tiles(const gb_lfc* l, const float* a, float* c, int64_t nx, cudaStream_t st);
+
 template <typename T>
 static int integrate_t(const gb_lfc* l, const void* a, void* c, int64_t nx, int q, cudaStream_t st,
                        int64_t per_q = 0) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (tiles_usable(l, a))
+      return integrate_tiles(l, static_cast<const float*>(a), static_cast<float*>(c), nx, st);
+  }
   // groups are sorted by nm on the host; one launch per padded class
   int g = 0;
   while (g < l->ngroups) {
@@ -557,10 +590,334 @@ static int add_nm(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cu
   return check_launch("lfc_add_kernel");
 }
 
+
+// ------------------------------------------------ brick-tiled FP32 (real)
+// The flattened grid is cut into 32-point chunks of four 8-point sub-tiles;
+// an entry is one (volume, sub-tile it touches) with the volume's values
+// there as a dense [m][p] 8 x 8 block.  A brick is a run of at most TBRICK
+// consecutive chunks with entries that meets at most TSLOTS function groups
+// (its slots) and holds at most TBENT entries.  One CTA takes one (brick,
+// group of 32 bands) and first copies into shared memory, with coalesced
+// 16-byte cp.async copies, the brick's rows of a (a band row pitch of
+// 32 TBRICK + 4 floats, so that lanes reading one band each do not collide
+// on banks), its entries' blocks and, for the add, the coefficients of its
+// slots as [slot][m][band] (rows of cT, c transposed by a first kernel).
+// Every operand of the FMAs then comes from shared memory.
+//  add:        warp w updates sub-tiles w, w + 8, ... in place (one owner per
+//              sub-tile): a[x][p] += sum_e sum_m A_e[m][p] c[x][M_e + m];
+//              the brick's rows are then written back.
+//  integrate:  warp s sums slot s over its entries (lists made on the host)
+//              and writes one partial sum per (brick, slot, band); a second
+//              kernel adds dv times each group's partials, in brick order,
+//              to c.
+// No atomics: the results do not depend on scheduling.
+constexpr int TCH = 32;                    // points per chunk
+constexpr int TSLOTS = 16;                 // function groups per brick
+constexpr int TBRICK = 8;                  // chunks per brick
+constexpr int TBENT = 192;                 // entries per brick
+constexpr int TBAND = 32;                  // bands per CTA
+constexpr int TPITCH = TBRICK * TCH + 4;   // floats per band row in shared memory
+constexpr int TADD_WARPS = 16;
+
+struct TileView {
+  const int* ch_c;      // [nch] chunk index (first point 32 c) of every used chunk
+  const int* ch_eoff;   // [4 nch + 1] entries of (chunk, sub-tile)
+  const int* e_info;    // [ne] slot | nm << 8
+  const float* e_A;     // [ne][8][8]
+  const int* br_ch0;    // [nbr + 1] chunk range of each brick
+  const int* br_pbase;  // [nbr + 1] first (brick, slot) pair of each brick
+  const int* ps_M;      // [npart] group of each (brick, slot): its first function
+  const int* ps_nm;     // [npart] and function count
+  const int* ps_eoff;   // [npart + 1] entries of each (brick, slot):
+  const int* ps_info;   //   (entry - first entry of the brick) | sub-tile << 16 | nm << 24
+};
+
+static TileView tile_view(const gb_lfc* l) {
+  return TileView{l->tch_c, l->tch_eoff, l->te_info, l->te_A, l->tbr_ch0, l->tbr_pbase,
+                  l->tps_M, l->tps_nm, l->tps_eoff, l->tps_info};
+}
+
+// shared-memory copy of brick b for bands x0 .. x0 + nb - 1 (of the rows at a)
+__device__ __forceinline__ void brick_stage(const TileView& t, int b, const float* __restrict__ a, int64_t nG,
+                                            int x0, int nb, float* sa, float* sA, float* sc,
+                                            const float* __restrict__ cT, int ldT) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int k0 = t.br_ch0[b], nk = t.br_ch0[b + 1] - k0;
+  for (int x = warp; x < nb; x += nw) {
+    const float* src = a + (int64_t)(x0 + x) * nG;
+    for (int i = lane; i < nk * 8; i += 32) {
+      const int kk = i >> 3, q = i & 7;
+      const int64_t G = (int64_t)t.ch_c[k0 + kk] * TCH + 4 * q;
+      float* d = sa + x * TPITCH + kk * TCH + 4 * q;
+      if (G < nG) cp_async16(d, src + G);
+      else *reinterpret_cast<float4*>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+  const int E0 = t.ch_eoff[4 * k0], E1 = t.ch_eoff[4 * (k0 + nk)];
+  for (int i = threadIdx.x; i < (E1 - E0) * 16; i += blockDim.x) cp_async16(sA + 4 * i, t.e_A + (int64_t)E0 * 64 + 4 * i);
+  if (sc) {
+    const int pbase = t.br_pbase[b], S = t.br_pbase[b + 1] - pbase;
+    for (int r = warp; r < S * 8; r += nw) {
+      const int s = r >> 3, m = r & 7;
+      if (lane < 8) {
+        float* d = sc + r * TBAND + 4 * lane;
+        if (m < t.ps_nm[pbase + s]) cp_async16(d, cT + (int64_t)(t.ps_M[pbase + s] + m) * ldT + x0 + 4 * lane);
+        else *reinterpret_cast<float4*>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+}
+
+__global__ void lfc_coef_transpose_kernel(const float* __restrict__ c, int nM, int R, int ldT, float* __restrict__ cT) {
+  __shared__ float tile[32][33];
+  const int M0 = blockIdx.x * 32, x0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int x = x0 + i, M = M0 + threadIdx.x;
+    tile[i][threadIdx.x] = (x < R && M < nM) ? c[(int64_t)x * nM + M] : 0.f;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int M = M0 + i;
+    if (M < nM) cT[(int64_t)M * ldT + x0 + threadIdx.x] = tile[threadIdx.x][i];
+  }
+}
+
+// acc (points 2k, 2k+1 in acc[k]) += A row m (4 float2) * cv
+__device__ __forceinline__ void add_row(float2 (&acc)[4], const float4* __restrict__ Ab, int m, float cv) {
+  const float4 A0 = Ab[2 * m], A1 = Ab[2 * m + 1];
+  const float2 c2 = make_float2(cv, cv);
+  acc[0] = __ffma2_rn(make_float2(A0.x, A0.y), c2, acc[0]);
+  acc[1] = __ffma2_rn(make_float2(A0.z, A0.w), c2, acc[1]);
+  acc[2] = __ffma2_rn(make_float2(A1.x, A1.y), c2, acc[2]);
+  acc[3] = __ffma2_rn(make_float2(A1.z, A1.w), c2, acc[3]);
+}
+
+__global__ void __launch_bounds__(32 * TADD_WARPS) lfc_add_tiles_kernel(const TileView t, const float* __restrict__ cT,
+                                                                       int ldT, float* __restrict__ a, int64_t nG,
+                                                                       int R, int sA_floats) {
+  extern __shared__ __align__(16) float tsm[];
+  float* sa = tsm;
+  float* sA = sa + TBAND * TPITCH;
+  float* sc = sA + sA_floats;
+  const int b = blockIdx.x, x0 = blockIdx.y * TBAND;
+  const int nb = min(TBAND, R - x0);
+  brick_stage(t, b, a, nG, x0, nb, sa, sA, sc, cT, ldT);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int k0 = t.br_ch0[b], nk = t.br_ch0[b + 1] - k0;
+  const int E0 = t.ch_eoff[4 * k0];
+  for (int st = warp; st < 4 * nk; st += TADD_WARPS) {
+    const int e0 = t.ch_eoff[4 * k0 + st], e1 = t.ch_eoff[4 * k0 + st + 1];
+    if (e0 == e1) continue;
+    float* row = sa + lane * TPITCH + 8 * st;
+    const float4 u = *reinterpret_cast<const float4*>(row), v = *reinterpret_cast<const float4*>(row + 4);
+    float2 acc[4] = {make_float2(u.x, u.y), make_float2(u.z, u.w), make_float2(v.x, v.y), make_float2(v.z, v.w)};
+    int info = t.e_info[e0];
+    for (int e = e0; e < e1; ++e) {
+      const int nm = info >> 8;
+      const float4* Ab = reinterpret_cast<const float4*>(sA + (e - E0) * 64);
+      const float* cs = sc + (info & 255) * 8 * TBAND + lane;
+      if (e + 1 < e1) info = t.e_info[e + 1];
+      if (nm == 8) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) add_row(acc, Ab, m, cs[m * TBAND]);
+      } else {
+        for (int m = 0; m < nm; ++m) add_row(acc, Ab, m, cs[m * TBAND]);
+      }
+    }
+    *reinterpret_cast<float4*>(row) = make_float4(acc[0].x, acc[0].y, acc[1].x, acc[1].y);
+    *reinterpret_cast<float4*>(row + 4) = make_float4(acc[2].x, acc[2].y, acc[3].x, acc[3].y);
+  }
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  for (int x = warp; x < nb; x += nw) {
+    float* dst = a + (int64_t)(x0 + x) * nG;
+    for (int i = lane; i < nk * 8; i += 32) {
+      const int kk = i >> 3, q = i & 7;
+      const int64_t G = (int64_t)t.ch_c[k0 + kk] * TCH + 4 * q;
+      if (G < nG)
+        *reinterpret_cast<float4*>(dst + G) = *reinterpret_cast<const float4*>(sa + x * TPITCH + kk * TCH + 4 * q);
+    }
+  }
+}
+
+// acc[m] (even / odd point sums) += A row m . av
+__device__ __forceinline__ void int_row(float2 (&acc)[8], const float4* __restrict__ Ab, int m, const float2 (&av)[4]) {
+  const float4 A0 = Ab[2 * m], A1 = Ab[2 * m + 1];
+  float2 s = acc[m];
+  s = __ffma2_rn(make_float2(A0.x, A0.y), av[0], s);
+  s = __ffma2_rn(make_float2(A0.z, A0.w), av[1], s);
+  s = __ffma2_rn(make_float2(A1.x, A1.y), av[2], s);
+  s = __ffma2_rn(make_float2(A1.z, A1.w), av[3], s);
+  acc[m] = s;
+}
+
+__global__ void __launch_bounds__(32 * TSLOTS) lfc_integrate_tiles_kernel(const TileView t,
+                                                                         const float* __restrict__ a, int64_t nG,
+                                                                         int R, float* __restrict__ part) {
+  extern __shared__ __align__(16) float tsm[];
+  float* sa = tsm;
+  float* sA = sa + TBAND * TPITCH;
+  const int b = blockIdx.x, x0 = blockIdx.y * TBAND;
+  const int nb = min(TBAND, R - x0);
+  brick_stage(t, b, a, nG, x0, nb, sa, sA, nullptr, nullptr, 0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pbase = t.br_pbase[b], S = t.br_pbase[b + 1] - pbase;
+  if (warp >= S) return;
+  float2 acc[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) acc[m] = make_float2(0.f, 0.f);
+  const int q0 = t.ps_eoff[pbase + warp], q1 = t.ps_eoff[pbase + warp + 1];
+  int info = q0 < q1 ? t.ps_info[q0] : 0;
+  for (int q = q0; q < q1; ++q) {
+    const int el = info & 0xffff, lst = (info >> 16) & 255, nm = info >> 24;
+    if (q + 1 < q1) info = t.ps_info[q + 1];
+    const float* row = sa + lane * TPITCH + 8 * lst;
+    const float4 u = *reinterpret_cast<const float4*>(row), v = *reinterpret_cast<const float4*>(row + 4);
+    const float2 av[4] = {make_float2(u.x, u.y), make_float2(u.z, u.w), make_float2(v.x, v.y), make_float2(v.z, v.w)};
+    const float4* Ab = reinterpret_cast<const float4*>(sA + el * 64);
+    if (nm == 8) {
+#pragma unroll
+      for (int m = 0; m < 8; ++m) int_row(acc, Ab, m, av);
+    } else {
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < nm) int_row(acc, Ab, m, av);
+    }
+  }
+  if (lane < nb) {
+    float4* d = reinterpret_cast<float4*>(part + ((int64_t)(pbase + warp) * R + x0 + lane) * 8);
+    d[0] = make_float4(acc[0].x + acc[0].y, acc[1].x + acc[1].y, acc[2].x + acc[2].y, acc[3].x + acc[3].y);
+    d[1] = make_float4(acc[4].x + acc[4].y, acc[5].x + acc[5].y, acc[6].x + acc[6].y, acc[7].x + acc[7].y);
+  }
+}
+
+// c[x][M_g + m] += dv sum of group g's partials (brick order)
+__global__ void lfc_tiles_reduce_kernel(const int* __restrict__ gr_M, const int* __restrict__ gr_nm,
+                                        const int* __restrict__ poff, const int* __restrict__ pidx,
+                                        const float* __restrict__ part, int R, float* __restrict__ c, int nM,
+                                        float dv) {
+  const int g = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= R * 8) return;
+  const int x = i >> 3, m = i & 7;
+  if (m >= gr_nm[g]) return;
+  // four independent sums (partials q, q + 4, ... in each) keep four loads
+  // in flight; they are combined in a fixed order
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  const int q0 = poff[g], q1 = poff[g + 1];
+  const float* pp = part + (int64_t)x * 8 + m;
+  const int64_t ps = (int64_t)R * 8;
+  int q = q0;
+  for (; q + 4 <= q1; q += 4) {
+    s0 += pp[pidx[q] * ps];
+    s1 += pp[pidx[q + 1] * ps];
+    s2 += pp[pidx[q + 2] * ps];
+    s3 += pp[pidx[q + 3] * ps];
+  }
+  for (; q < q1; ++q) s0 += pp[pidx[q] * ps];
+  float* cp = c + (int64_t)x * nM + gr_M[g] + m;
+  *cp = fmaf(dv, (s0 + s1) + (s2 + s3), *cp);
+}
+
+// grow the work space (never inside stream capture)
+static int tile_work(const gb_lfc* l, size_t bytes, cudaStream_t st) {
+  if (bytes <= l->work_bytes) return GB_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return fail(GB_E_INVALID, "lfc: the tiled FP32 path needs a larger work space; make one call of this size "
+                              "before capturing it in a graph");
+  if (l->work) {
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_launch("lfc work space");
+    cudaFree(l->work);
+    l->work = nullptr;
+    l->work_bytes = 0;
+  }
+  if (cudaMalloc(&l->work, bytes) != cudaSuccess) {
+    l->work = nullptr;
+    return fail(GB_E_NOMEM, "lfc: work space allocation failed");
+  }
+  l->work_bytes = bytes;
+  return GB_OK;
+}
+
+static int tile_smem_attr() {
+  static int done = 0;
+  if (!done) {
+    const int mx = (TBAND * TPITCH + TBENT * 64 + TSLOTS * 8 * TBAND) * (int)sizeof(float);
+    if (cudaFuncSetAttribute(lfc_add_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+        cudaFuncSetAttribute(lfc_integrate_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
+            cudaSuccess)
+      return check_launch("lfc tiled shared memory");
+    done = 1;
+  }
+  return GB_OK;
+}
+
+// usable for this call: FP32 real data, rows 16-byte aligned
+static bool tiles_usable(const gb_lfc* l, const void* a) {
+  return l->tiled && (reinterpret_cast<uintptr_t>(a) & 15) == 0;
+}
+
+// passes of at most 256 bands bound the work space
+static int add_tiles(const gb_lfc* l, const float* c, float* a, int64_t nx, cudaStream_t st) {
+  if (l->tbr_n == 0) return GB_OK;
+  int rc = tile_smem_attr();
+  if (rc) return rc;
+  const int Rmax = (int)std::min<int64_t>(nx, 256);
+  rc = tile_work(l, (size_t)l->nM * ((Rmax + 31) / 32 * 32) * sizeof(float), st);
+  if (rc) return rc;
+  float* cT = static_cast<float*>(l->work);
+  const int sA_floats = l->tbr_emax * 64;
+  const int smem = (TBAND * TPITCH + sA_floats + TSLOTS * 8 * TBAND) * (int)sizeof(float);
+  for (int64_t x0 = 0; x0 < nx; x0 += 256) {
+    const int R = (int)std::min<int64_t>(nx - x0, 256);
+    const int ldT = (R + 31) / 32 * 32;
+    dim3 tg((unsigned)((l->nM + 31) / 32), (unsigned)(ldT / 32));
+    lfc_coef_transpose_kernel<<<tg, dim3(32, 8), 0, st>>>(c + x0 * l->nM, l->nM, R, ldT, cT);
+    dim3 grid((unsigned)l->tbr_n, (unsigned)(ldT / TBAND));
+    lfc_add_tiles_kernel<<<grid, 32 * TADD_WARPS, smem, st>>>(tile_view(l), cT, ldT, a + x0 * l->nG, l->nG, R,
+                                                              sA_floats);
+    rc = check_launch("lfc_add_tiles_kernel");
+    if (rc) return rc;
+  }
+  return GB_OK;
+}
+
+static int integrate_tiles(const gb_lfc* l, const float* a, float* c, int64_t nx, cudaStream_t st) {
+  if (l->tbr_n == 0) return GB_OK;
+  int rc = tile_smem_attr();
+  if (rc) return rc;
+  const int Rmax = (int)std::min<int64_t>(nx, 256);
+  rc = tile_work(l, (size_t)l->tpart_n * Rmax * 8 * sizeof(float), st);
+  if (rc) return rc;
+  float* part = static_cast<float*>(l->work);
+  const int smem = (TBAND * TPITCH + l->tbr_emax * 64) * (int)sizeof(float);
+  for (int64_t x0 = 0; x0 < nx; x0 += 256) {
+    const int R = (int)std::min<int64_t>(nx - x0, 256);
+    dim3 grid((unsigned)l->tbr_n, (unsigned)((R + TBAND - 1) / TBAND));
+    lfc_integrate_tiles_kernel<<<grid, 32 * l->tbr_smax, smem, st>>>(tile_view(l), a + x0 * l->nG, l->nG, R, part);
+    rc = check_launch("lfc_integrate_tiles_kernel");
+    if (rc) return rc;
+    dim3 rg((unsigned)((R * 8 + 255) / 256), (unsigned)l->ngroups);
+    lfc_tiles_reduce_kernel<<<rg, 256, 0, st>>>(l->gr_M, l->gr_nm, l->tgr_poff, l->tgr_pidx, part, R,
+                                                c + x0 * l->nM, l->nM, (float)l->dv);
+    rc = check_launch("lfc_tiles_reduce_kernel");
+    if (rc) return rc;
+  }
+  return GB_OK;
+}
+
+
 template <typename T>
 static int add_t(const gb_lfc* l, const void* c, void* a, int64_t nx, int q, cudaStream_t st,
                  int64_t per_q = 0) {
   if (l->P == 0) return GB_OK;
+  if constexpr (std::is_same<T, float>::value) {
+    if (tiles_usable(l, a)) return add_tiles(l, static_cast<const float*>(c), static_cast<float*>(a), nx, st);
+  }
   if constexpr (!Elem<T>::cplx) {
     if (l->fast_nmax) return add_fast<T>(l, c, a, nx, st);
   }
@@ -713,6 +1070,7 @@ extern "C" {
 
 int gb_lfc_free(gb_lfc* l) {
   if (!l) return GB_OK;
+  if (l->work) cudaFree(l->work);
   for (void* p : l->allocations) cudaFree(p);
   delete l;
   return GB_OK;
@@ -825,6 +1183,121 @@ int gb_lfc_new(int nW, const double* A_all, const int64_t* ngm_W, const int* nm_
     l->full32 = full32;
     l->full64 = full64;
   }
+  // brick tiling for the FP32 real path
+  std::vector<int> tch_c, tch_eoff, te_nm, te_slot, te_lst, te_info, tbr_ch0, tbr_pbase, tps_M, tps_nm, tps_eoff,
+      tps_info, tgr_poff, tgr_pidx;
+  std::vector<float> te_A;
+  int tbr_smax = 1, tbr_emax = 0;
+  bool tiled = l->maxnm <= 8 && nG % 4 == 0 && nW > 0;
+  if (tiled) {
+    const int ngr = (int)gr_M.size();
+    std::vector<int> vol_group(nW);
+    for (int gi = 0; gi < ngr; ++gi)
+      for (int v = gr_voff[gi]; v < gr_voff[gi + 1]; ++v) vol_group[gv_W[v]] = gi;
+    // entries: (sub-tile, volume) with their blocks
+    struct Ent { int64_t st; int W; int64_t blk; };
+    std::vector<Ent> ents;
+    std::vector<float> blocks;
+    for (int W = 0; W < nW; ++W) {
+      int64_t last = -1;
+      for (int64_t r = row0[W]; r < row0[W + 1]; ++r) {
+        const int64_t G = row_G[r];
+        if (G / 8 != last) {
+          last = G / 8;
+          ents.push_back({last, W, (int64_t)(blocks.size() / 64)});
+          blocks.resize(blocks.size() + 64, 0.f);
+        }
+        float* b = blocks.data() + ents.back().blk * 64;
+        for (int m = 0; m < nm_W[W]; ++m)
+          b[m * 8 + (int)(G % 8)] = (float)A_all[aoff[W] + (r - row0[W]) * nm_W[W] + m];
+      }
+    }
+    std::sort(ents.begin(), ents.end(),
+              [](const Ent& x, const Ent& y) { return x.st != y.st ? x.st < y.st : x.W < y.W; });
+    std::vector<int> te_g;   // group of every entry
+    tch_eoff.push_back(0);
+    for (size_t i = 0; i < ents.size();) {
+      const int64_t ch = ents[i].st / 4;
+      tch_c.push_back((int)ch);
+      for (int j = 0; j < 4; ++j) {
+        for (; i < ents.size() && ents[i].st == ch * 4 + j; ++i) {
+          te_nm.push_back(nm_W[ents[i].W]);
+          te_g.push_back(vol_group[ents[i].W]);
+          te_A.insert(te_A.end(), blocks.begin() + ents[i].blk * 64, blocks.begin() + ents[i].blk * 64 + 64);
+        }
+        tch_eoff.push_back((int)te_nm.size());
+      }
+    }
+    const size_t ne = te_nm.size();
+    te_slot.assign(ne, 0);
+    te_lst.assign(ne, 0);
+    // bricks: <= TBRICK consecutive chunks, <= TSLOTS groups, <= TBENT entries
+    std::vector<int> slot_of(ngr, -1), brick_groups, newg;
+    std::vector<std::vector<int>> group_parts(ngr);
+    tbr_ch0.push_back(0);
+    tbr_pbase.push_back(0);
+    tps_eoff.push_back(0);
+    auto close_brick = [&](int end_chunk) {
+      const int b0 = tbr_ch0.back();
+      const int E0 = tch_eoff[4 * b0], E1 = tch_eoff[4 * end_chunk];
+      for (size_t k = 0; k < brick_groups.size(); ++k) {
+        const int g = brick_groups[k];
+        group_parts[g].push_back(tbr_pbase.back() + (int)k);
+        tps_M.push_back(gr_M[g]);
+        tps_nm.push_back(gr_nm[g]);
+        for (int e = E0; e < E1; ++e)
+          if (te_slot[e] == (int)k) tps_info.push_back((e - E0) | te_lst[e] << 16 | te_nm[e] << 24);
+        tps_eoff.push_back((int)tps_info.size());
+        slot_of[g] = -1;
+      }
+      tbr_smax = std::max(tbr_smax, (int)brick_groups.size());
+      tbr_emax = std::max(tbr_emax, E1 - E0);
+      tbr_pbase.push_back(tbr_pbase.back() + (int)brick_groups.size());
+      tbr_ch0.push_back(end_chunk);
+      brick_groups.clear();
+    };
+    auto chunk_groups = [&](size_t ci, bool only_new) {
+      newg.clear();
+      for (int e = tch_eoff[4 * ci]; e < tch_eoff[4 * ci + 4]; ++e) {
+        const int g = te_g[e];
+        if ((!only_new || slot_of[g] < 0) && std::find(newg.begin(), newg.end(), g) == newg.end()) newg.push_back(g);
+      }
+    };
+    for (size_t ci = 0; ci < tch_c.size(); ++ci) {
+      const int nent = tch_eoff[4 * ci + 4] - tch_eoff[4 * ci];
+      chunk_groups(ci, true);
+      const int in_brick = (int)ci - tbr_ch0.back();
+      if (in_brick > 0 && (in_brick == TBRICK || brick_groups.size() + newg.size() > (size_t)TSLOTS ||
+                           tch_eoff[4 * ci + 4] - tch_eoff[4 * tbr_ch0.back()] > TBENT)) {
+        close_brick((int)ci);
+        chunk_groups(ci, false);
+      }
+      if (newg.size() > (size_t)TSLOTS || nent > TBENT) {
+        tiled = false;   // one chunk is too crowded: keep the point-major kernels
+        break;
+      }
+      for (int g : newg) {
+        slot_of[g] = (int)brick_groups.size();
+        brick_groups.push_back(g);
+      }
+      const int kk = (int)ci - tbr_ch0.back();
+      for (int j = 0; j < 4; ++j)
+        for (int e = tch_eoff[4 * ci + j]; e < tch_eoff[4 * ci + j + 1]; ++e) {
+          te_slot[e] = slot_of[te_g[e]];
+          te_lst[e] = 4 * kk + j;
+        }
+    }
+    if (tiled) {
+      close_brick((int)tch_c.size());
+      te_info.resize(ne);
+      for (size_t e = 0; e < ne; ++e) te_info[e] = te_slot[e] | te_nm[e] << 8;
+      tgr_poff.push_back(0);
+      for (int gi = 0; gi < ngr; ++gi) {
+        tgr_pidx.insert(tgr_pidx.end(), group_parts[gi].begin(), group_parts[gi].end());
+        tgr_poff.push_back((int)tgr_pidx.size());
+      }
+    }
+  }
   l->ngroups = (int)gr_M.size();
   l->h_gr_nm = gr_nm;
   l->P = (int64_t)pt_G.size();
@@ -861,6 +1334,18 @@ int gb_lfc_new(int nW, const double* A_all, const int64_t* ngm_W, const int* nm_
       ok = cudaDeviceSynchronize() == cudaSuccess;
     }
   }
+  if (ok && tiled) {
+    ok = upload(l, &l->tch_c, tch_c) && upload(l, &l->tch_eoff, tch_eoff) && upload(l, &l->te_info, te_info) &&
+         upload(l, &l->te_A, te_A) && upload(l, &l->tbr_ch0, tbr_ch0) && upload(l, &l->tbr_pbase, tbr_pbase) &&
+         upload(l, &l->tps_M, tps_M) && upload(l, &l->tps_nm, tps_nm) && upload(l, &l->tps_eoff, tps_eoff) &&
+         upload(l, &l->tps_info, tps_info) &&
+         upload(l, &l->tgr_poff, tgr_poff) && upload(l, &l->tgr_pidx, tgr_pidx);
+    l->tiled = ok;
+    l->tbr_n = (int)tbr_ch0.size() - 1;
+    l->tbr_smax = tbr_smax;
+    l->tbr_emax = tbr_emax;
+    l->tpart_n = tbr_pbase.back();
+  }
   if (!ok) {
     gb_lfc_free(l);
     return fail(GB_E_NOMEM, "gb_lfc_new: device allocation / upload failed");
@@ -868,6 +1353,8 @@ int gb_lfc_new(int nW, const double* A_all, const int64_t* ngm_W, const int* nm_
   *out = l;
   return GB_OK;
 }
+
+int gb_lfc_tiled(const gb_lfc* l) { return l && l->tiled ? 1 : 0; }
 
 int gb_lfc_add(const gb_lfc* l, const void* c_xM, void* a_xG, int64_t nx, int dtype, int q, void* stream) {
   GB_REQUIRE(l && dtype_valid(dtype) && nx >= 0, "gb_lfc_add: bad arguments");

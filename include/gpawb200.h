@@ -245,6 +245,15 @@ int gb_lfc_add(const gb_lfc* lfc, const void* c_xM, void* a_xG, int64_t nx,
 int gb_lfc_integrate(const gb_lfc* lfc, const void* a_xG, void* c_xM,
                      int64_t nx, int dtype, int q, void* stream);
 int gb_lfc_free(gb_lfc* lfc);
+/* FP32 real data (q = -1): where every volume has at most 8 functions, nG
+ * is a multiple of 4 and no 32-point chunk of the grid meets more than 16
+ * function groups, add and integrate run chunk-tiled and keep a work space
+ * on the object (nM x 256 floats for add, a few MB of partial sums for
+ * integrate).  It grows on the first call of a larger band count, which
+ * must not be inside stream capture; calls on one object are ordered on
+ * one stream.  gb_lfc_tiled returns 1 when the object has that path (a
+ * query of this implementation; no reference counterpart). */
+int gb_lfc_tiled(const gb_lfc* lfc);
 /* add / integrate over nk k-point groups of the nx rows in one launch:
  * row x takes the Bloch phases of k-point q = x / (nx / nk) (complex
  * dtypes; nk <= nq). */

@@ -282,3 +282,69 @@ def test_add_all_bands_equals_band_blocks():
     for x in range(0, nx, 10):
         lfc.add_M(b2[x:x + 10], c[x:x + 10].contiguous())
     assert torch.equal(b, b2)
+
+
+def _tiled_case(natoms, n_c, rc_ang, nfun=8, seed=9):
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.lfc import LFC
+    from gpaw_b200.spline import Spline
+    bohr = 0.52917721
+    rc = rc_ang / bohr
+    r = np.linspace(0, rc, 61)
+    ls = {1: [0], 4: [0, 1], 8: [0, 1, 0, 1]}[nfun]
+    spl = [(l, rc, np.exp(-(r / (0.9 / bohr))**2) * (1 + 0.3 * j)) for j, l in enumerate(ls)]
+    gd = GridDescriptor(n_c, np.array(n_c) * 0.2 / bohr, True)
+    spos = np.random.default_rng(seed).random((natoms, 3))
+    lfc = LFC(gd, [[Spline.from_data(*s) for s in spl]] * natoms)
+    lfc.set_positions(spos)
+    Phi = ol.dense_functions(gd.N_c, gd.cell_cv, gd.pbc_c, spos, [spl] * natoms)
+    return gd, lfc, Phi
+
+
+@pytest.mark.parametrize('natoms,n_c,rc,nfun', [
+    (10, (20, 22, 26), 1.6, 8),   # 11440 points: the last 32-point chunk is partial
+    (36, (24, 24, 24), 1.1, 4),   # <= 14 groups per chunk, bricks split at 16
+    (9, (16, 20, 18), 1.4, 1),    # one function per atom
+])
+@pytest.mark.parametrize('nx', [1, 37, 300])
+def test_fp32_tiled_add_integrate(natoms, n_c, rc, nfun, nx):
+    """The chunk-tiled FP32 add / integrate (gb_lfc_tiled objects) against
+    the oracle's dense sums within 1e-5, band counts of one pass (1, 37) and
+    of two (300 = 256 + 44); deterministic (two integrates are equal), band
+    blocks of 10 equal to one call, and add / integrate adjoint."""
+    from gpaw_b200 import _native as nat
+    gd, lfc, Phi = _tiled_case(natoms, n_c, rc, nfun)
+    assert nat.lib().gb_lfc_tiled(lfc.lfc.handle) == 1
+    rng = np.random.default_rng(nx)
+    c = rng.standard_normal((nx, lfc.Mmax))
+    a0 = rng.standard_normal((nx,) + tuple(gd.n_c))
+    want_add = ol.add(a0.copy(), c, Phi)
+    want_int = ol.integrate(a0, Phi, gd.dv)
+    b = torch.from_numpy(a0).cuda().float()
+    c32 = torch.from_numpy(c).cuda().float()
+    lfc.add_M(b, c32)
+    assert rel(b.double().cpu().numpy(), want_add) < 1e-5
+    a32 = torch.from_numpy(a0).cuda().float()
+    cM = lfc.integrate(a32, {})
+    assert rel(cM.double().cpu().numpy(), want_int) < 1e-5
+    assert torch.equal(lfc.integrate(a32, {}), cM)
+    b2 = torch.from_numpy(a0).cuda().float()
+    for x in range(0, nx, 10):
+        lfc.add_M(b2[x:x + 10], c32[x:x + 10].contiguous())
+    assert torch.equal(b2, b)
+    cM2 = torch.cat([lfc.integrate(a32[x:x + 10], {}) for x in range(0, nx, 10)])
+    assert torch.equal(cM2, cM)
+
+
+def test_fp32_tiled_fallback_when_a_chunk_meets_too_many_groups():
+    """More than 16 function groups over one 32-point chunk: the object keeps
+    the point-major kernels, with the same results."""
+    from gpaw_b200 import _native as nat
+    gd, lfc, Phi = _tiled_case(40, (16, 16, 16), 3.0, nfun=1)
+    assert nat.lib().gb_lfc_tiled(lfc.lfc.handle) == 0
+    rng = np.random.default_rng(1)
+    c = rng.standard_normal((5, lfc.Mmax))
+    a0 = rng.standard_normal((5,) + tuple(gd.n_c))
+    b = torch.from_numpy(a0).cuda().float()
+    lfc.add_M(b, torch.from_numpy(c).cuda().float())
+    assert rel(b.double().cpu().numpy(), ol.add(a0.copy(), c, Phi)) < 1e-5
