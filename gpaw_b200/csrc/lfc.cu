@@ -794,32 +794,40 @@ __global__ void __launch_bounds__(32 * TSLOTS) lfc_integrate_tiles_kernel(const 
   }
 }
 
-// c[x][M_g + m] += dv sum of group g's partials (brick order)
-__global__ void lfc_tiles_reduce_kernel(const int* __restrict__ gr_M, const int* __restrict__ gr_nm,
-                                        const int* __restrict__ poff, const int* __restrict__ pidx,
-                                        const float* __restrict__ part, int R, float* __restrict__ c, int nM,
-                                        float dv) {
+// c[x][M_g + m] += dv sum of group g's partials.  A CTA takes 32 outputs
+// (x, m) of one group -- four bands -- and eight slices of its partial list:
+// thread (slice s, output o) sums partials s, s + 8, ... (32 consecutive
+// floats per partial: coalesced), then the eight sums are added in slice
+// order.  Fixed order throughout: results do not depend on scheduling.
+__global__ void __launch_bounds__(256) lfc_tiles_reduce_kernel(const int* __restrict__ gr_M,
+                                                              const int* __restrict__ gr_nm,
+                                                              const int* __restrict__ poff,
+                                                              const int* __restrict__ pidx,
+                                                              const float* __restrict__ part, int R,
+                                                              float* __restrict__ c, int nM, float dv) {
+  __shared__ float red[8][33];
   const int g = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= R * 8) return;
-  const int x = i >> 3, m = i & 7;
-  if (m >= gr_nm[g]) return;
-  // four independent sums (partials q, q + 4, ... in each) keep four loads
-  // in flight; they are combined in a fixed order
-  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-  const int q0 = poff[g], q1 = poff[g + 1];
-  const float* pp = part + (int64_t)x * 8 + m;
-  const int64_t ps = (int64_t)R * 8;
-  int q = q0;
-  for (; q + 4 <= q1; q += 4) {
-    s0 += pp[pidx[q] * ps];
-    s1 += pp[pidx[q + 1] * ps];
-    s2 += pp[pidx[q + 2] * ps];
-    s3 += pp[pidx[q + 3] * ps];
+  const int o = threadIdx.x & 31, sl = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + o;              // output (x, m) = (i / 8, i % 8)
+  float s = 0.f;
+  if (i < R * 8) {
+    const float* pp = part + i;
+    const int64_t ps = (int64_t)R * 8;
+    const int q1 = poff[g + 1];
+    for (int q = poff[g] + sl; q < q1; q += 8) s += pp[pidx[q] * ps];
   }
-  for (; q < q1; ++q) s0 += pp[pidx[q] * ps];
-  float* cp = c + (int64_t)x * nM + gr_M[g] + m;
-  *cp = fmaf(dv, (s0 + s1) + (s2 + s3), *cp);
+  red[sl][o] = s;
+  __syncthreads();
+  if (sl == 0 && i < R * 8) {
+    const int x = i >> 3, m = i & 7;
+    if (m < gr_nm[g]) {
+      float t = red[0][o];
+#pragma unroll
+      for (int k = 1; k < 8; ++k) t += red[k][o];
+      float* cp = c + (int64_t)x * nM + gr_M[g] + m;
+      *cp = fmaf(dv, t, *cp);
+    }
+  }
 }
 
 // grow the work space (never inside stream capture)
@@ -901,7 +909,7 @@ static int integrate_tiles(const gb_lfc* l, const float* a, float* c, int64_t nx
     lfc_integrate_tiles_kernel<<<grid, 32 * l->tbr_smax, smem, st>>>(tile_view(l), a + x0 * l->nG, l->nG, R, part);
     rc = check_launch("lfc_integrate_tiles_kernel");
     if (rc) return rc;
-    dim3 rg((unsigned)((R * 8 + 255) / 256), (unsigned)l->ngroups);
+    dim3 rg((unsigned)((R * 8 + 31) / 32), (unsigned)l->ngroups);
     lfc_tiles_reduce_kernel<<<rg, 256, 0, st>>>(l->gr_M, l->gr_nm, l->tgr_poff, l->tgr_pidx, part, R,
                                                 c + x0 * l->nM, l->nM, (float)l->dv);
     rc = check_launch("lfc_tiles_reduce_kernel");
