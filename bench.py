@@ -150,14 +150,20 @@ def time_launches(fn, reps, stream):
     return float(np.mean([a.elapsed_time(b) for a, b in ev]))
 
 
-def suite(torch, stream):
-    """GB/s of the other kernel-microbench kernels (algorithmic bytes)."""
+SUITE_PARTS = ('grid', 'lfc', 'xc', 'vcycle')
+
+
+def suite(torch, stream, nb=None, parts=SUITE_PARTS):
+    """GB/s of the other kernel-microbench kernels (algorithmic bytes); nb
+    grids per call (default: the benchmark's 256); parts: any of 'grid'
+    (stencils and transfers), 'lfc', 'xc', 'vcycle'."""
+    NB = nb or globals()['NB']
     from gpaw_b200.fd_operators import Laplace, Gradient
     from gpaw_b200.transformers import Transformer
     from gpaw_b200.preconditioner import Preconditioner
     out = {}
     g = torch.Generator(device='cuda').manual_seed(1)
-    for dtype, dname in ((torch.float64, 'f64'), (torch.float32, 'f32')):
+    for dtype, dname in ((torch.float64, 'f64'), (torch.float32, 'f32')) if 'grid' in parts else ():
         for pbc in (True, False):
             gd = grid(pbc)
             x = torch.randn((NB,) + tuple(gd.n_c), generator=g, device='cuda', dtype=dtype)
@@ -192,6 +198,16 @@ def suite(torch, stream):
                     out[f'interpolate_k{2 * nn}_{dname}_{bc}'] = round(rbytes / t / 1e6, 1)
                 del xf, xc, yf
             del x, y
+    if 'lfc' in parts:
+        suite_lfc(torch, stream, NB, g, out)
+    if 'xc' in parts:
+        suite_xc(torch, stream, g, out)
+    if 'vcycle' in parts:
+        suite_vcycle(torch, stream, g, out)
+    return out
+
+
+def suite_lfc(torch, stream, NB, g, out):
     # LFC add / integrate: 64 atom-centred Gaussians x (l = 0, 1, 2) with
     # cutoff 2.5 A on the 96^3 grid (h = 0.2 A), 256 bands, FP64
     from gpaw_b200.lfc import LFC
@@ -222,9 +238,10 @@ def suite(torch, stream):
     out['lfc_integrate_f64_64atoms_256bands_ms'] = round(t, 3)
     out['lfc_integrate_f64_GBps'] = round(NB * npts * 8 / t / 1e6, 1)
     out['lfc_covered_points'] = npts
-    del a, cM, c_axi, lfc
+
+
+def suite_xc(torch, stream, g, out):
     # XC on the fine grid of the H2O-cluster config (151^3), FP64
-    from gpaw_b200.grid_descriptor import GridDescriptor
     from gpaw_b200.xc import XCKernel
     ng = 151**3
     n_g = torch.rand((1, ng), generator=g, device='cuda', dtype=torch.float64) + 1e-3
@@ -239,8 +256,13 @@ def suite(torch, stream):
         call()
         t = time_launches(call, 5, stream)
         out[f'xc_{name}_151cubed_GBps'] = round(arrays * ng * 8 / t / 1e6, 1)
+
+
+def suite_vcycle(torch, stream, g, out):
     # V-cycle on 160 bands of the Si64 grid (56^3, periodic), FP64
     from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.fd_operators import Laplace
+    from gpaw_b200.preconditioner import Preconditioner
     gd = GridDescriptor((56, 56, 56), (20.52, 20.52, 20.52), True)
     kin = Laplace(gd, -0.5, 3)
     P = Preconditioner(gd, kin, float, block=10)
@@ -250,7 +272,6 @@ def suite(torch, stream):
     t = time_launches(lambda: P(R, out=d), 5, stream)
     out['precond_vcycle_f64_56cubed_160bands_ms'] = round(t, 3)
     out['precond_vcycle_f64_min_bytes_GBps'] = round(2 * R.numel() * 8 / t / 1e6, 1)
-    return out
 
 
 def scf_benchmark(train_steps=400):
@@ -655,6 +676,11 @@ def main():
                          'shapes (160 FP32 bands x 56^3 points): Gram matrix and '
                          'subspace rotation, next to the FP64 / SIMT GEMMs they '
                          'replace (the command line used for ncu captures)')
+    ap.add_argument('--suite-only', action='store_true',
+                    help='run the kernel suite alone with --bands grids per call '
+                         '(the command line used for ncu captures of its kernels)')
+    ap.add_argument('--suite-part', action='append', choices=SUITE_PARTS,
+                    help='with --suite-only: only these parts (repeatable)')
     ap.add_argument('--dtype', default='f64', choices=['f64', 'f32'],
                     help='storage precision of the kernel-only run (the '
                          'benchmark line itself is FP64)')
@@ -675,6 +701,12 @@ def main():
         return
     if args.band_gemm_only:
         band_gemm_benchmark(args)
+        return
+    if args.suite_only:
+        import torch
+        parts = tuple(args.suite_part or SUITE_PARTS)
+        print(json.dumps({'suite_GBps': suite(torch, torch.cuda.current_stream(), args.bands, parts),
+                          'bands': args.bands}))
         return
 
     import torch
