@@ -310,8 +310,44 @@ def gradient_stencil(h_cv, v, scale=1.0, n=1):
 
 def Laplace(gd, scale=1.0, n=1, dtype=float, xp=None):
     if n == 9:
-        raise NotImplementedError('FTLaplace (n=9) is not part of this build')
+        return FTLaplace(gd, scale, dtype)
     return GUCLaplace(gd, scale, n, dtype, xp=xp)
+
+
+class FTLaplace:
+    """The spectral Laplacian that Laplace(gd, scale, n=9) returns
+    (gpaw/fd_operators.py:357-382): on a periodic grid,
+    out = Re F^-1[-scale |k|^2 F[in]] with k the reciprocal-lattice vectors of
+    the FFT frequencies (folded to -N/2 .. N/2 - 1 per axis), applied to all
+    leading (band) dimensions at once through cuFFT (torch.fft).  Like the
+    reference it keeps the real part, and its diagonal element is
+    6 / h_00^2 whatever the scale."""
+
+    def __init__(self, gd, scale=1.0, dtype=float, xp=None):
+        if not np.all(gd.pbc_c):
+            raise ValueError('FTLaplace needs a periodic grid')
+        N_c = np.asarray(gd.N_c)
+        i_cq = np.indices(tuple(N_c)).reshape(3, -1)
+        half = (N_c // 2)[:, None]
+        i_cq = (i_cq + half) % N_c[:, None] - half
+        k_vq = (2.0 * np.pi * gd.icell_cv.T) @ i_cq
+        k2 = -scale * (k_vq**2).sum(0).reshape(tuple(N_c))
+        self.gd = gd
+        self.k2_Q = torch.as_tensor(k2, dtype=torch.float64, device=gd.device)
+        self.d = 6.0 / gd.h_cv[0, 0]**2
+        self.npoints = 1000
+        self.description = 'FFT Laplacian'
+
+    def apply(self, in_xg, out_xg, phase_cd=None):
+        if not in_xg.is_cuda:
+            raise nat.GPAWB200Error('FTLaplace.apply needs CUDA tensors')
+        f = torch.fft.fftn(in_xg.to(torch.complex128), dim=(-3, -2, -1))
+        y = torch.fft.ifftn(f * self.k2_Q, dim=(-3, -2, -1)).real
+        out_xg.copy_(y.to(out_xg.dtype) if not out_xg.dtype.is_complex else y)
+        return out_xg
+
+    def get_diagonal_element(self):
+        return self.d
 
 
 class GUCLaplace(FDOperator):

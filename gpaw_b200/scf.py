@@ -129,6 +129,19 @@ class PulayMixer:
         return (alpha.to(N.dtype) @ (N + self.beta * P)).reshape(nin_G.shape)
 
 
+def _append_log_line(path, it, log, graphed):
+    """One JSON object per iteration (JSON Lines): iteration, total energy
+    (eV), eigenstate error (eV^2 per electron), density change (electrons
+    per electron), wall time since the start (s), whether the iteration was
+    a graph replay and the iteration of a learned-preconditioner fallback."""
+    import json
+    rec = {'iteration': it, 'energy_eV': log.energies[-1], 'eigenstate_error': log.errors[-1],
+           'density_change': log.ddens[-1], 'time_s': round(log.times[-1], 6),
+           'graphed': bool(graphed), 'fallback_at': log.fallback_at or None}
+    with open(path, 'a') as f:
+        f.write(json.dumps(rec) + '\n')
+
+
 @dataclass
 class SCFLog:
     energies: list = field(default_factory=list)
@@ -421,7 +434,7 @@ class Calculation:
         self.eigensolver.preconditioner = pc
 
     def run(self, maxiter=200, energy_tol=1e-5, density_tol=1e-4,
-            eigenstates_tol=4e-8, callback=None, graph=False):
+            eigenstates_tol=4e-8, callback=None, graph=False, logfile=None):
         """Iterate to convergence: energy change (eV / valence electron)
         over the last 3 iterations < energy_tol, density change per
         electron < density_tol, eigenstate error (eV^2 / electron) <
@@ -474,6 +487,8 @@ class Calculation:
             log.ddens.append(ddens)
             log.times.append(time.perf_counter() - t0)
             log.iterations = it
+            if logfile is not None:
+                _append_log_line(logfile, it, log, step is not None)
             if callback:
                 callback(self, it, log)
             if it >= 3:
