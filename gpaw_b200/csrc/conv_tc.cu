@@ -3,28 +3,44 @@
 // counterpart; the network stands in for the V-cycle of
 // c/fd_preconditioner.c).
 //
-//   y[b][co][p] = sum_{ci < 16} sum_{k < 27} w[co][ci][k] x[b][ci][p + o_k]
+//   y[b][co][z][p] = sum_{ci < 16} sum_{dz, dy, dx} w[co][ci][dz][dy][dx]
+//                                  x[b][ci][z + dz - 1][p + (dy - 1, dx - 1)]
 //
-// as an implicit GEMM without im2col: a CTA keeps the input planes
-// z - 1 .. z + 1 of one band (a ring of four slots, the next plane staged
-// while the current one's MMAs run), padded by the periodic halo, in the canonical
-// K-major no-swizzle layout of the MMA -- [channel quad][padded point][4
-// channels], 16 bytes per point, so a core matrix is 8 consecutive points
-// (SBO = 128 bytes) and the two channel quads of a K = 8 step are one quad
-// stride apart (LBO).  A tap (dz, dy, dx) is then the same operand with its
-// start address moved by the tap's linear offset in the padded block, and
-// the output plane is ceil(P1 P2 / 128) tiles of 128 consecutive padded
-// points (halo points are computed and dropped):
-//   D[128 points][16 co] += A_tap[128 points][8 ci] . W_tap[16 co][8 ci]^T
-// with tcgen05.mma.cta_group::1.kind::tf32 (M = 128, N = 16, K = 8) issued
-// by one thread per (tile, channel half) -- up to four threads, each with its
-// own accumulator, since a single thread cannot issue these small MMAs fast
-// enough -- 27 taps x 2 products per pair.  The
-// weights are BF16 and therefore exact TF32 numbers; the activations are
-// split x = hi + lo (RN TF32 parts) so the products keep FP32 accuracy.
-// The accumulators (TMEM, 2 x 16 columns per tile) are read back with
-// tcgen05.ld.32x32b by warps 4-7 (one padded point per lane) and the
-// interior points are written, 16 channels each.  Waits are bounded.
+// as an implicit GEMM without im2col.  The flattened output planes (band,
+// z) are cut into ranges of at most `per` planes, one range per CTA (two
+// CTAs per SM, the whole grid in one wave for the Si64 shape).  A CTA walks
+// the INPUT planes of its range in order (z_lo - 1 .. z_hi per band
+// segment, periodic in z), each staged once into one of two shared-memory
+// slots -- padded by the periodic (y, x) halo, split x = hi + lo into RN TF32
+// parts, in the canonical K-major no-swizzle layout of the MMA:
+// [channel quad][padded point][4 channels], 16 bytes per point, so a core
+// matrix is 8 consecutive points (SBO = 128 bytes) and the two channel quads
+// of a K = 8 step are one quad stride apart (LBO).  An in-plane tap (dy, dx)
+// is the same operand with its start address moved by the tap's offset in
+// the padded plane.
+//
+// The three z taps are folded into N: the B operand of tap (dy, dx) has 48
+// rows n = 16 k + co holding w[co][ci][2 - k][dy][dx], and one input plane
+// z_in contributes, through one MMA per (tap, channel half, hi / lo), to the
+// accumulators of output planes z_in - 1 + k, k = 0, 1, 2.  Output plane o
+// of the range owns TMEM columns 16 o .. 16 o + 15 of each 128-point tile,
+// so the three accumulators of an input plane are 48 adjacent columns:
+//   D[128 points][16 (o .. o + 2)][16 co] += A_tap[128 points][8 ci] . B_tap[48][8 ci]^T
+// (tcgen05.mma.cta_group::1.kind::tf32, M = 128, N = 48; N = 16 or 32 at
+// the ends of a segment, where fewer output planes are wanted).  Each A
+// tile is read from shared memory 36 times per input plane for 48
+// accumulator columns, against 108 times for 16 columns when every z tap
+// is its own MMA; TMEM is zeroed once, every MMA accumulates.  The weights
+// are BF16 and therefore exact TF32 numbers; hi and lo products keep FP32
+// accuracy.
+//
+// Per input plane: one thread per tile (lane 0 of warps 0-1) issues the
+// tile's 36 MMAs and commits them to an mbarrier; warps 4-7 meanwhile read
+// back (tcgen05.ld.32x32b, one padded point per lane) the output plane that
+// the previous input plane completed and store its interior points, and
+// warps 2-7 stage the next input plane into the other slot.  Thread 0 alone
+// waits on the mbarrier (bounded; a timeout sets the error flag and ends
+// the CTA's loop), the rest of the CTA at the barrier that follows.
 #include <algorithm>
 #include <cuda_bf16.h>
 #include "internal.cuh"
@@ -48,44 +64,78 @@ int conv_tc_error_flag(int clear) {
 namespace {
 using namespace tc;
 
+constexpr int CT_THREADS = 256;
+constexpr int CT_STAGERS = 192;          // warps 2-7
+constexpr int CT_WROWS = 48;             // B rows per tap: (k, co)
+constexpr int CT_WFLOATS = 9 * 4 * CT_WROWS * 4;
+
 struct ConvTcArgs {
   const float* x;                 // (nb, 16, n0, n1, n2)
   float* y;                       // (nb, cout, n0, n1, n2)
   const __nv_bfloat16* w;         // [cout][16][27]
-  int64_t nb;
+  int64_t total;                  // nb n0 output planes
   int cout, n0, n1, n2;
-  int P1, P2, PP, tiles, margin, npts, zchunk, accumulate, nissue;
+  int P2, PP, tiles, margin, npts, per, accumulate, nissue;
   uint32_t ncols;
 };
 
-__device__ __forceinline__ float rn_tf32_(float x) {
-  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+// one input plane of a CTA's walk
+struct Item {
+  int64_t band;
+  int zs;        // plane of x (periodic)
+  int kl, kh;    // z taps k = kl .. kh feed output planes z_in - 1 + k
+  int obase;     // range-local index of output plane z_in - 1 + kl
+  int done;      // range-local output plane complete after this item (-1: none)
+};
+
+constexpr int CT_MAXITEMS = 24;         // 3 per: every segment adds two halo planes
+
+// the input planes a CTA walks for output planes [g0, g1): per band segment
+// z_lo .. z_hi - 1 of outputs, the inputs z_lo - 1 .. z_hi; returns the count
+__device__ int build_items(const ConvTcArgs& a, int64_t g0, int64_t g1, Item* items) {
+  int n = 0;
+  for (int64_t g = g0; g < g1;) {
+    const int64_t band = g / a.n0;
+    const int zlo = (int)(g - band * a.n0);
+    const int zhi = (int)(g1 - g < (int64_t)(a.n0 - zlo) ? zlo + (g1 - g) : a.n0);
+    for (int i = 0; i < zhi - zlo + 2 && n < CT_MAXITEMS; ++i, ++n) {
+      const int zin = zlo - 1 + i;
+      const int lo = max(zlo, zin - 1), hi = min(zhi - 1, zin + 1);
+      Item& it = items[n];
+      it.band = band;
+      it.zs = zin < 0 ? zin + a.n0 : (zin >= a.n0 ? zin - a.n0 : zin);
+      it.kl = lo - zin + 1;
+      it.kh = hi - zin + 1;
+      it.obase = (int)(g - g0) + (lo - zlo);
+      it.done = i >= 2 ? (int)(g - g0) + (i - 2) : -1;
+    }
+    g += zhi - zlo;
+  }
+  return n;
 }
 
-// shared-memory descriptor without swizzle (layout type 0)
-__device__ __forceinline__ uint64_t sdesc_none(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  return sdesc(saddr, lbo, sbo, 0u);
-}
-
-// ring of 4 staged planes (each with its own margins): the MMAs of plane z
-// read the slots of z - 1, z, z + 1 while the CTA stages plane z + 2 into
-// the fourth
-__global__ void __launch_bounds__(256, 1) conv16_tc_kernel(const ConvTcArgs a) {
+__global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcArgs a) {
   extern __shared__ __align__(128) unsigned char ctc_smem[];
-  float* sW = reinterpret_cast<float*>(ctc_smem);              // [27][4][16][4]
-  float* Xhi = sW + 27 * 4 * 16 * 4;                            // [4 slots][4 quads][npts][4]
-  float* Xlo = Xhi + 4 * 4 * a.npts * 4;
-  uint64_t* done = reinterpret_cast<uint64_t*>(Xlo + 4 * 4 * a.npts * 4);
+  float* sW = reinterpret_cast<float*>(ctc_smem);              // [9 taps][4 quads][48 rows][4]
+  float* Xhi = sW + CT_WFLOATS;                                 // [2 slots][4 quads][npts][4]
+  float* Xlo = Xhi + 2 * 4 * a.npts * 4;
+  uint64_t* done = reinterpret_cast<uint64_t*>(Xlo + 2 * 4 * a.npts * 4);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  int* sfail = reinterpret_cast<int*>(tslot + 1);
+  int* snit = sfail + 1;
+  Item* items = reinterpret_cast<Item*>(done + 3);           // [CT_MAXITEMS]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2, P2 = a.P2, PP = a.PP;
+  const int64_t g0 = (int64_t)blockIdx.x * a.per, g1 = min(a.total, g0 + a.per);
 
-  for (int e = tid; e < 27 * 256; e += blockDim.x) {
-    const int tap = e >> 8, r = e & 255, q = r >> 6, co = (r >> 2) & 15, i = r & 3;
-    sW[e] = co < a.cout ? __bfloat162float(a.w[(co * 16 + 4 * q + i) * 27 + tap]) : 0.f;
+  for (int e = tid; e < CT_WFLOATS; e += CT_THREADS) {
+    const int tap = e / (4 * CT_WROWS * 4), r = e % (4 * CT_WROWS * 4);
+    const int q = r / (CT_WROWS * 4), n = (r >> 2) % CT_WROWS, i = r & 3;
+    const int k = n >> 4, co = n & 15;
+    sW[e] = co < a.cout ? __bfloat162float(a.w[(co * 16 + 4 * q + i) * 27 + 9 * (2 - k) + tap]) : 0.f;
   }
-  // margins of every slot and quad: zero (only dropped halo outputs read them)
-  for (int e = tid; e < 16 * 2 * a.margin; e += blockDim.x) {
+  // margins of both slots and every quad: zero (only dropped halo outputs read them)
+  for (int e = tid; e < 8 * 2 * a.margin; e += CT_THREADS) {
     const int sq = e / (2 * a.margin), m = e % (2 * a.margin);
     const int pt = m < a.margin ? m : a.margin + PP + (m - a.margin);
     reinterpret_cast<float4*>(Xhi)[sq * a.npts + pt] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -94,136 +144,151 @@ __global__ void __launch_bounds__(256, 1) conv16_tc_kernel(const ConvTcArgs a) {
   if (tid == 0) {
     mbar_init(done, a.nissue);
     mbar_fence_init();
+    *sfail = 0;
+    *snit = build_items(a, g0, g1, items);
   }
   if (warp == 1) {
     tmem_alloc(tslot, a.ncols);
     tmem_relinquish();
   }
-  const int64_t b = blockIdx.y;
   const int64_t nplane = (int64_t)n1 * n2, nvol = nplane * n0;
-  const float* xb = a.x + b * 16 * nvol;
-  const int z_beg = blockIdx.x * a.zchunk, z_end = min(z_beg + a.zchunk, n0);
-  auto slot_of = [&](int p) { return (p - z_beg + 1) & 3; };
-  // stage input plane p (periodic) into its slot, split hi / lo
-  // (all of a thread's loads for a plane are issued before any is used:
-  // up to 8 x 4 values in flight instead of one L2 round trip per 4)
-  auto stage = [&](int p) {
-    constexpr int MAXIT = 8;
-    const int sl = slot_of(p);
-    const int zs = p < 0 ? p + n0 : (p >= n0 ? p - n0 : p);
-    for (int e0 = tid; e0 < 4 * PP; e0 += MAXIT * 256) {
-      float v[MAXIT][4];
+  // stage the input plane of `it` into slot `sl`, split hi / lo (warps 2-7):
+  // a thread takes padded points r, r + 192 (one index division each) and
+  // loads all 16 channels of both before it writes any
+  auto stage = [&](const Item& it, int sl) {
+    const float* xb = a.x + it.band * 16 * nvol + it.zs * nplane;
+    for (int r0 = tid - 64; r0 < PP; r0 += 2 * CT_STAGERS) {
+      float v[2][16];
 #pragma unroll
-      for (int it = 0; it < MAXIT; ++it) {
-        const int e = e0 + it * 256;
-        if (e < 4 * PP) {
-          const int q = e / PP, r = e % PP, yy = r / P2, xx = r % P2;
+      for (int j = 0; j < 2; ++j) {
+        const int r = r0 + j * CT_STAGERS;
+        if (r < PP) {
+          const int yy = r / P2, xx = r - yy * P2;
           int ys = yy - 1, xs = xx - 1;
           ys = ys < 0 ? ys + n1 : (ys >= n1 ? ys - n1 : ys);
           xs = xs < 0 ? xs + n2 : (xs >= n2 ? xs - n2 : xs);
-          const float* src = xb + (int64_t)(4 * q) * nvol + zs * nplane + (int64_t)ys * n2 + xs;
+          const float* src = xb + (int64_t)ys * n2 + xs;
 #pragma unroll
-          for (int i = 0; i < 4; ++i) v[it][i] = __ldg(src + i * nvol);
+          for (int c = 0; c < 16; ++c) v[j][c] = __ldg(src + c * nvol);
         }
       }
 #pragma unroll
-      for (int it = 0; it < MAXIT; ++it) {
-        const int e = e0 + it * 256;
-        if (e < 4 * PP) {
-          const int q = e / PP, r = e % PP;
-          float h[4], l[4];
+      for (int j = 0; j < 2; ++j) {
+        const int r = r0 + j * CT_STAGERS;
+        if (r < PP) {
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            h[i] = rn_tf32_(v[it][i]);
-            l[i] = rn_tf32_(v[it][i] - h[i]);
+          for (int q = 0; q < 4; ++q) {
+            float h[4], l[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              h[i] = rn_tf32(v[j][4 * q + i]);
+              l[i] = rn_tf32(v[j][4 * q + i] - h[i]);
+            }
+            const int pt = (sl * 4 + q) * a.npts + a.margin + r;
+            reinterpret_cast<float4*>(Xhi)[pt] = make_float4(h[0], h[1], h[2], h[3]);
+            reinterpret_cast<float4*>(Xlo)[pt] = make_float4(l[0], l[1], l[2], l[3]);
           }
-          const int pt = (sl * 4 + q) * a.npts + a.margin + r;
-          reinterpret_cast<float4*>(Xhi)[pt] = make_float4(h[0], h[1], h[2], h[3]);
-          reinterpret_cast<float4*>(Xlo)[pt] = make_float4(l[0], l[1], l[2], l[3]);
         }
       }
     }
   };
-  stage(z_beg - 1);
-  stage(z_beg);
-  if (z_beg + 1 < z_end + 1) stage(z_beg + 1);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(16 >> 3) << 17) |
-                         ((uint32_t)(128 >> 4) << 24);
+  // store output plane `o` (range-local) of every tile (warps 4-7)
+  auto epilogue = [&](int o) {
+    const int64_t g = g0 + o, band = g / n0;
+    const int z = (int)(g - band * n0);
+    const int q4 = warp & 3;
+    for (int t = 0; t < a.tiles; ++t) {
+      uint32_t r[16];
+      tmem_ld16(tmem + (uint32_t)(16 * (t * a.per + o)) + ((uint32_t)(32 * q4) << 16), r);
+      tmem_wait_ld();
+      const int lin = t * 128 + 32 * q4 + lane;          // padded point of the plane
+      const int yy = lin / P2, xx = lin % P2;
+      if (lin < PP && yy >= 1 && yy <= n1 && xx >= 1 && xx <= n2) {
+        float* yp = a.y + (band * a.cout) * nvol + z * nplane + (int64_t)(yy - 1) * n2 + (xx - 1);
+        for (int co = 0; co < a.cout; ++co) {
+          const float v = __uint_as_float(r[co]);
+          if (a.accumulate) yp[co * nvol] += v;
+          else yp[co * nvol] = v;
+        }
+      }
+    }
+  };
+  const int nit = *snit;
+  if (warp >= 4) {
+    for (uint32_t c = 0; c < a.ncols; c += 16) tmem_st16_zero(tmem + c + ((uint32_t)(32 * (warp & 3)) << 16));
+    tmem_wait_st();
+  }
+  if (warp >= 2 && nit > 0) stage(items[0], 0);
+  const uint32_t idesc0 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(128 >> 4) << 24);
   const uint32_t qstride = (uint32_t)a.npts * 16u;
   uint32_t phase = 0;
-  bool ok = true;
-  for (int z = z_beg; z < z_end; ++z) {
+  for (int i = 0; i < nit; ++i) {
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    if (*sfail) break;
     if (warp < a.nissue && lane == 0) {
-      // issuer w (warps 0 .. nissue - 1) feeds the (tile, channel half)
-      // pairs w, w + nissue, ...; every pair has its own accumulator
-      // (columns 16 (2 t + c)), so the issuers are independent and each
-      // commits to `done` (nissue arrivals).  Descriptors differ only in the
-      // start address (bits 0-13, 16-byte units, addresses < 256 KB): three
-      // base descriptors plus offsets.
-      const uint64_t ah0 = sdesc_none(su32(Xhi), qstride, 128);
-      const uint64_t al0 = sdesc_none(su32(Xlo), qstride, 128);
-      const uint64_t bw0 = sdesc_none(su32(sW), 256, 128);
-      const uint32_t npts = (uint32_t)a.npts;
-      uint32_t sbase[3];
-#pragma unroll
-      for (int dz = 0; dz < 3; ++dz) sbase[dz] = (uint32_t)(slot_of(z + dz - 1) * 4) * npts;
+      // issuer w feeds tiles w, w + nissue, ... (one accumulator set per
+      // tile, so each tile's MMAs come from one thread, in order); the
+      // descriptors differ only in the start address (bits 0-13, 16-byte
+      // units, addresses < 256 KB)
+      const Item& it = items[i];
+      const uint32_t N = 16u * (uint32_t)(it.kh - it.kl + 1);
+      const uint32_t idesc = idesc0 | ((N >> 3) << 17);
+      const uint64_t ah0 = sdesc(su32(Xhi), qstride, 128, 0u);
+      const uint64_t al0 = sdesc(su32(Xlo), qstride, 128, 0u);
+      const uint64_t bw0 = sdesc(su32(sW), CT_WROWS * 16, 128, 0u) + (uint64_t)(16 * it.kl);
+      const uint32_t sbase = (uint32_t)((i & 1) * 4 * a.npts);
       const int rowoff[3] = {-P2, 0, P2};
-      for (int pr = warp; pr < 2 * a.tiles; pr += a.nissue) {
-        const int t = pr >> 1, c = pr & 1;
-        const uint32_t d = tmem + 16u * pr;
+      for (int t = warp; t < a.tiles; t += a.nissue) {
+        const uint32_t d = tmem + (uint32_t)(16 * (t * a.per + it.obase));
         const int tb = a.margin + t * 128;
 #pragma unroll
-        for (int tap = 0; tap < 27; ++tap) {
-          const uint32_t off = sbase[tap / 9] + (uint32_t)(tb + rowoff[(tap / 3) % 3] + (tap % 3 - 1));
-          const uint64_t delta = off + 2u * c * npts;
-          const uint64_t bw = bw0 + (uint64_t)(tap * 64 + c * 32);
-          mma_tf32(d, ah0 + delta, bw, idesc, tap > 0 ? 1u : 0u);
-          mma_tf32(d, al0 + delta, bw, idesc, 1u);
+        for (int tap = 0; tap < 9; ++tap) {
+          const uint32_t off = sbase + (uint32_t)(tb + rowoff[tap / 3] + (tap % 3 - 1));
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const uint64_t delta = off + 2u * c * (uint32_t)a.npts;
+            const uint64_t bw = bw0 + (uint64_t)(tap * 4 * CT_WROWS + c * 2 * CT_WROWS);
+            mma_tf32(d, ah0 + delta, bw, idesc, 1u);
+            mma_tf32(d, al0 + delta, bw, idesc, 1u);
+          }
         }
       }
       mma_commit(done);
     }
-    // the next plane's input goes to the slot plane z - 2 used
-    if (z + 2 < z_end + 1) stage(z + 2);
-    if (warp >= 4) {
-      if (ok && !mbar_wait(done, phase)) {
-        ok = false;
-        atomicCAS(&g_conv_tc_error, 0, 301);
-      }
-      tc_fence_after();
-      const int q4 = warp & 3;
-      for (int t = 0; t < a.tiles; ++t) {
-        uint32_t r[16], r1[16];
-        tmem_ld16(tmem + 32u * t + ((uint32_t)(32 * q4) << 16), r);
-        tmem_ld16(tmem + 32u * t + 16u + ((uint32_t)(32 * q4) << 16), r1);
-        tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 16; ++i) r[i] = __float_as_uint(__uint_as_float(r[i]) + __uint_as_float(r1[i]));
-        const int lin = t * 128 + 32 * q4 + lane;          // padded point of the plane
-        const int yy = lin / P2, xx = lin % P2;
-        if (ok && lin < PP && yy >= 1 && yy <= n1 && xx >= 1 && xx <= n2) {
-          float* yp = a.y + (b * a.cout) * nvol + z * nplane + (int64_t)(yy - 1) * n2 + (xx - 1);
-          for (int co = 0; co < a.cout; ++co) {
-            const float v = __uint_as_float(r[co]);
-            if (a.accumulate) yp[co * nvol] += v;
-            else yp[co * nvol] = v;
-          }
-        }
-      }
-      tc_fence_before();
-    } else if (warp < a.nissue) {
-      // the MMAs must be complete before the ring advances past their slots
-      if (ok && !mbar_wait(done, phase)) ok = false;
+    // the output plane the previous input plane completed (its columns are
+    // not among those this plane's MMAs write)
+    if (warp >= 4 && i > 0) {
+      const int o = items[i - 1].done;
+      if (o >= 0) epilogue(o);
+    }
+    // the next input plane goes to the slot the previous plane's MMAs read
+    if (warp >= 2 && i + 1 < nit) stage(items[i + 1], (i + 1) & 1);
+    // one thread waits for this plane's MMAs; the others wait at the next
+    // barrier, which issues no instructions (a spinning CTA starves the
+    // staging warps of issue slots)
+    if (tid == 0 && !mbar_wait(done, phase)) {
+      atomicCAS(&g_conv_tc_error, 0, 301);
+      *sfail = 1;
     }
     phase ^= 1u;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (*sfail) {
+    // MMAs may still be in flight: give them a bounded wait before the
+    // accumulators are freed
+    if (tid == 0) mbar_wait(done, phase ^ 1u);
+  } else if (warp >= 4 && nit > 0) {
+    const int o = items[nit - 1].done;
+    if (o >= 0) epilogue(o);
   }
   tc_fence_before();
   __syncthreads();
@@ -239,40 +304,41 @@ __global__ void __launch_bounds__(256, 1) conv16_tc_kernel(const ConvTcArgs a) {
 int conv16_tc_try(const float* x, const void* w_bf16, float* y, int64_t nb, int cout, int n0, int n1, int n2,
                   int accumulate, cudaStream_t st, int* launched) {
   *launched = 0;
-  if (cout < 1 || cout > 16 || nb < 1 || nb > 65535 || n0 < 2 || n1 < 2 || n2 < 2) return GB_OK;
+  if (cout < 1 || cout > 16 || nb < 1 || n0 < 2 || n1 < 2 || n2 < 2) return GB_OK;
   ConvTcArgs a;
   a.x = x;
   a.y = y;
   a.w = reinterpret_cast<const __nv_bfloat16*>(w_bf16);
-  a.nb = nb;
+  a.total = nb * n0;
   a.cout = cout;
   a.n0 = n0; a.n1 = n1; a.n2 = n2;
-  a.P1 = n1 + 2;
   a.P2 = n2 + 2;
-  a.PP = a.P1 * a.P2;
+  a.PP = (n1 + 2) * a.P2;
   a.tiles = (a.PP + 127) / 128;
-  if (a.tiles * 32 > 512) return GB_OK;
+  if (a.tiles > 16) return GB_OK;
   const int m = std::max(a.P2 + 1, a.tiles * 128 - a.PP + a.P2 + 1);
   a.margin = (m + 7) / 8 * 8;
   a.npts = a.PP + 2 * a.margin;                   // one slot of one quad
   if (a.npts > 16383) return GB_OK;
-  // three plane chunks per band (measured best of 1..7 chunks on 14^3 x 160)
-  a.zchunk = std::max(1, std::min(n0, (n0 + 2) / 3));
+  // output planes per CTA: 16 TMEM columns each per tile, at most 256
+  // columns so that two CTAs share an SM
+  a.per = std::min(8, 256 / (16 * a.tiles));
+  const int64_t nblk = (a.total + a.per - 1) / a.per;
+  if (nblk > 0x7fffffff) return GB_OK;
   a.accumulate = accumulate;
-  a.nissue = std::min(4, 2 * a.tiles);            // MMA-issuing threads (warps 0-3)
+  a.nissue = std::min(2, a.tiles);
   uint32_t nc = 32;
-  while (nc < (uint32_t)(32 * a.tiles)) nc *= 2;
-  if (nc > 512) return GB_OK;
+  while (nc < (uint32_t)(16 * a.tiles * a.per)) nc *= 2;
   a.ncols = nc;
-  const size_t smem = (size_t)(27 * 256 + 2 * 4 * 4 * a.npts * 4) * sizeof(float) + 64;
+  const size_t smem = (size_t)(CT_WFLOATS + 2 * 2 * 4 * a.npts * 4) * sizeof(float) + 24 +
+                      CT_MAXITEMS * sizeof(Item);
   if (smem > 220 * 1024) return GB_OK;
   static size_t attr = 0;
   if (smem > attr) {
     cudaFuncSetAttribute(conv16_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = smem;
   }
-  const dim3 grid((unsigned)((n0 + a.zchunk - 1) / a.zchunk), (unsigned)nb);
-  conv16_tc_kernel<<<grid, 256, smem, st>>>(a);
+  conv16_tc_kernel<<<(unsigned)nblk, CT_THREADS, smem, st>>>(a);
   *launched = 1;
   return check_launch("conv16_tc_kernel");
 }
