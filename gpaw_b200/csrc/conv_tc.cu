@@ -72,7 +72,9 @@ constexpr int CT_WFLOATS = 9 * 4 * CT_WROWS * 4;
 struct ConvTcArgs {
   const float* x;                 // (nb, 16, n0, n1, n2)
   float* y;                       // (nb, cout, n0, n1, n2)
-  const __nv_bfloat16* w;         // [cout][16][27]
+  const __nv_bfloat16* w;         // [cout][16][27] (plain convolution)
+  const float* G;                 // [16][6][6][6] (parity mode)
+  int parity;                     // 1: the parity mode (below)
   int64_t total;                  // nb n0 output planes
   int cout, n0, n1, n2;
   int P2, PP, tiles, margin, npts, per, accumulate, nissue;
@@ -131,8 +133,18 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
   for (int e = tid; e < CT_WFLOATS; e += CT_THREADS) {
     const int tap = e / (4 * CT_WROWS * 4), r = e % (4 * CT_WROWS * 4);
     const int q = r / (CT_WROWS * 4), n = (r >> 2) % CT_WROWS, i = r & 3;
-    const int k = n >> 4, co = n & 15;
-    sW[e] = co < a.cout ? __bfloat162float(a.w[(co * 16 + 4 * q + i) * 27 + 9 * (2 - k) + tap]) : 0.f;
+    const int k = n >> 4, co = n & 15, ci = 4 * q + i;
+    if (a.parity) {
+      // rows 0-7: TF32 high part of the parity-co weights, rows 8-15: the low part
+      const int par = co & 7;
+      const int tx = (par >> 2) - 2 * (1 - k) + 2, ty = ((par >> 1) & 1) - 2 * (tap / 3 - 1) + 2;
+      const int tz = (par & 1) - 2 * (tap % 3 - 1) + 2;
+      const float g = (tx < 5 && ty < 5 && tz < 5) ? __ldg(a.G + ci * 216 + (tx * 6 + ty) * 6 + tz) : 0.f;
+      const float h = rn_tf32(g);
+      sW[e] = co < 8 ? h : rn_tf32(g - h);
+    } else {
+      sW[e] = co < a.cout ? __bfloat162float(a.w[(co * 16 + ci) * 27 + 9 * (2 - k) + tap]) : 0.f;
+    }
   }
   // margins of both slots and every quad: zero (only dropped halo outputs read them)
   for (int e = tid; e < 8 * 2 * a.margin; e += CT_THREADS) {
@@ -208,11 +220,21 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
       const int lin = t * 128 + 32 * q4 + lane;          // padded point of the plane
       const int yy = lin / P2, xx = lin % P2;
       if (lin < PP && yy >= 1 && yy <= n1 && xx >= 1 && xx <= n2) {
-        float* yp = a.y + (band * a.cout) * nvol + z * nplane + (int64_t)(yy - 1) * n2 + (xx - 1);
-        for (int co = 0; co < a.cout; ++co) {
-          const float v = __uint_as_float(r[co]);
-          if (a.accumulate) yp[co * nvol] += v;
-          else yp[co * nvol] = v;
+        if (a.parity) {
+          // fine grid (2 n0, 2 n1, 2 n2): point 2 J + par gets high + low part
+          const int64_t f2 = 2 * n2, fpl = 4 * nplane;
+          float* yp = a.y + band * 8 * nvol + (int64_t)(2 * z) * fpl + (int64_t)(2 * (yy - 1)) * f2 + 2 * (xx - 1);
+#pragma unroll
+          for (int par = 0; par < 8; ++par)
+            yp[(par >> 2) * fpl + ((par >> 1) & 1) * f2 + (par & 1)] +=
+                __uint_as_float(r[par]) + __uint_as_float(r[par + 8]);
+        } else {
+          float* yp = a.y + (band * a.cout) * nvol + z * nplane + (int64_t)(yy - 1) * n2 + (xx - 1);
+          for (int co = 0; co < a.cout; ++co) {
+            const float v = __uint_as_float(r[co]);
+            if (a.accumulate) yp[co * nvol] += v;
+            else yp[co * nvol] = v;
+          }
         }
       }
     }
@@ -301,16 +323,10 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
 }  // namespace
 
 // plan and launch; 0 (not launched) when the layout does not apply
-int conv16_tc_try(const float* x, const void* w_bf16, float* y, int64_t nb, int cout, int n0, int n1, int n2,
-                  int accumulate, cudaStream_t st, int* launched) {
+static int conv_tc_launch(ConvTcArgs a, int64_t nb, int n0, int n1, int n2, cudaStream_t st, int* launched) {
   *launched = 0;
-  if (cout < 1 || cout > 16 || nb < 1 || n0 < 2 || n1 < 2 || n2 < 2) return GB_OK;
-  ConvTcArgs a;
-  a.x = x;
-  a.y = y;
-  a.w = reinterpret_cast<const __nv_bfloat16*>(w_bf16);
+  if (a.cout < 1 || a.cout > 16 || nb < 1 || n0 < 2 || n1 < 2 || n2 < 2) return GB_OK;
   a.total = nb * n0;
-  a.cout = cout;
   a.n0 = n0; a.n1 = n1; a.n2 = n2;
   a.P2 = n2 + 2;
   a.PP = (n1 + 2) * a.P2;
@@ -325,7 +341,6 @@ int conv16_tc_try(const float* x, const void* w_bf16, float* y, int64_t nb, int 
   a.per = std::min(8, 256 / (16 * a.tiles));
   const int64_t nblk = (a.total + a.per - 1) / a.per;
   if (nblk > 0x7fffffff) return GB_OK;
-  a.accumulate = accumulate;
   a.nissue = std::min(2, a.tiles);
   uint32_t nc = 32;
   while (nc < (uint32_t)(16 * a.tiles * a.per)) nc *= 2;
@@ -340,7 +355,40 @@ int conv16_tc_try(const float* x, const void* w_bf16, float* y, int64_t nb, int 
   }
   conv16_tc_kernel<<<(unsigned)nblk, CT_THREADS, smem, st>>>(a);
   *launched = 1;
-  return check_launch("conv16_tc_kernel");
+  return check_launch(a.parity ? "conv16_tc_kernel(parity)" : "conv16_tc_kernel");
+}
+
+int conv16_tc_try(const float* x, const void* w_bf16, float* y, int64_t nb, int cout, int n0, int n1, int n2,
+                  int accumulate, cudaStream_t st, int* launched) {
+  ConvTcArgs a{};
+  a.x = x;
+  a.y = y;
+  a.w = reinterpret_cast<const __nv_bfloat16*>(w_bf16);
+  a.cout = cout;
+  a.accumulate = accumulate;
+  return conv_tc_launch(a, nb, n0, n1, n2, st, launched);
+}
+
+// Parity mode (the coarse part of level 1 of the folded learned
+// preconditioner, as in fold_parity16_kernel):
+//   y[2J + par] += sum_c sum_{e in {-1,0,1}^3} G[c][par - 2e + 2] xc[c][J + e]
+// on the coarse grid (n0, n1, n2), y the fine grid (2 n0, 2 n1, 2 n2),
+// par in {0,1}^3 (axis 0 the slowest), tap index 5 (odd parity, e = -1)
+// zero.  It is the 16-channel convolution above with the eight parities as
+// output channels; G is FP32 (composite weights, not TF32 numbers), so B
+// rows 8-15 carry the TF32 low parts of rows 0-7 and the epilogue adds the
+// two accumulators: every product of the hi / lo parts of both operands is
+// formed, FP32 accuracy with no extra MMA.
+int conv_parity_tc_try(const float* xc, const float* G, float* y, int64_t nb, int n0, int n1, int n2,
+                       cudaStream_t st, int* launched) {
+  ConvTcArgs a{};
+  a.x = xc;
+  a.y = y;
+  a.G = G;
+  a.parity = 1;
+  a.cout = 16;
+  a.accumulate = 1;
+  return conv_tc_launch(a, nb, n0, n1, n2, st, launched);
 }
 
 }  // namespace gb

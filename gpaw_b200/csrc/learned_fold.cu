@@ -37,6 +37,12 @@
 #include "internal.cuh"
 
 namespace gb {
+
+// the parity convolution on the tensor cores (conv_tc.cu); *launched = 0
+// when the grid does not fit its layout
+int conv_parity_tc_try(const float* xc, const float* G, float* y, int64_t nb, int n0, int n1, int n2,
+                       cudaStream_t st, int* launched);
+
 namespace {
 
 // periodic index for -n <= x < 2n (every offset these kernels form stays in
@@ -656,6 +662,10 @@ int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* x
     // fine 5^3 part, then the coarse part added as a parity convolution
     int rc = launch_fine(fold_fine_kernel<2, 0>, a, "fold_fine_kernel<2,0>", st);
     if (rc) return rc;
+    // on the tensor cores when the coarse plane fits their layout
+    int launched = 0;
+    rc = conv_parity_tc_try(xc, G, y, nb, (int)(n_c[0] / 2), (int)(n_c[1] / 2), (int)(n_c[2] / 2), st, &launched);
+    if (rc || launched) return rc;
     const int m12 = (int)(n_c[1] / 2 * (n_c[2] / 2));
     const unsigned threads = (unsigned)std::min(256, (m12 + 31) / 32 * 32);
     fold_parity16_kernel<<<dim3((unsigned)(n_c[0] / 2), (unsigned)nb), threads, 0, st>>>(a);
