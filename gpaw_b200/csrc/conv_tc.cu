@@ -73,8 +73,8 @@ struct ConvTcArgs {
   const float* x;                 // (nb, 16, n0, n1, n2)
   float* y;                       // (nb, cout, n0, n1, n2)
   const __nv_bfloat16* w;         // [cout][16][27] (plain convolution)
-  const float* G;                 // [16][6][6][6] (parity mode)
-  int parity;                     // 1: the parity mode (below)
+  const float* G;                 // parity modes: [16][6][6][6] (1) or [5][5][5] (2)
+  int parity;                     // 0: plain; 1, 2: the parity modes (below)
   int64_t total;                  // nb n0 output planes
   int cout, n0, n1, n2;
   int P2, PP, tiles, margin, npts, per, accumulate, nissue;
@@ -135,11 +135,21 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
     const int q = r / (CT_WROWS * 4), n = (r >> 2) % CT_WROWS, i = r & 3;
     const int k = n >> 4, co = n & 15, ci = 4 * q + i;
     if (a.parity) {
-      // rows 0-7: TF32 high part of the parity-co weights, rows 8-15: the low part
+      // rows 0-7: TF32 high part of the parity-co weights, rows 8-15: the
+      // low part; e = (1 - k, tap / 3 - 1, tap % 3 - 1) the coarse offset
       const int par = co & 7;
-      const int tx = (par >> 2) - 2 * (1 - k) + 2, ty = ((par >> 1) & 1) - 2 * (tap / 3 - 1) + 2;
-      const int tz = (par & 1) - 2 * (tap % 3 - 1) + 2;
-      const float g = (tx < 5 && ty < 5 && tz < 5) ? __ldg(a.G + ci * 216 + (tx * 6 + ty) * 6 + tz) : 0.f;
+      const int e0 = 1 - k, e1 = tap / 3 - 1, e2 = tap % 3 - 1;
+      float g = 0.f;
+      if (a.parity == 1) {
+        const int tx = (par >> 2) - 2 * e0 + 2, ty = ((par >> 1) & 1) - 2 * e1 + 2, tz = (par & 1) - 2 * e2 + 2;
+        if (tx < 5 && ty < 5 && tz < 5) g = __ldg(a.G + ci * 216 + (tx * 6 + ty) * 6 + tz);
+      } else if (ci < 8) {
+        // fine offset d = 2 e + p' - par of input parity p' = ci
+        const int d0 = 2 * e0 + (ci >> 2) - (par >> 2), d1 = 2 * e1 + ((ci >> 1) & 1) - ((par >> 1) & 1);
+        const int d2 = 2 * e2 + (ci & 1) - (par & 1);
+        if (d0 >= -2 && d0 <= 2 && d1 >= -2 && d1 <= 2 && d2 >= -2 && d2 <= 2)
+          g = __ldg(a.G + ((d0 + 2) * 5 + (d1 + 2)) * 5 + (d2 + 2));
+      }
       const float h = rn_tf32(g);
       sW[e] = co < 8 ? h : rn_tf32(g - h);
     } else {
@@ -167,8 +177,12 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
   // stage the input plane of `it` into slot `sl`, split hi / lo (warps 2-7):
   // a thread takes padded points r, r + 192 (one index division each) and
   // loads all 16 channels of both before it writes any
+  const bool gather8 = a.parity == 2;
   auto stage = [&](const Item& it, int sl) {
-    const float* xb = a.x + it.band * 16 * nvol + it.zs * nplane;
+    // channel c of a plain input: x[band][c][zs]; the eight parity channels
+    // p' of a fine input (2 n0, 2 n1, 2 n2): x[band][2 zs + p'0][2 ys + p'1][2 xs + p'2]
+    const float* xb = gather8 ? a.x + it.band * 8 * nvol + (int64_t)(2 * it.zs) * 4 * nplane
+                              : a.x + it.band * 16 * nvol + it.zs * nplane;
     for (int r0 = tid - 64; r0 < PP; r0 += 2 * CT_STAGERS) {
       float v[2][16];
 #pragma unroll
@@ -179,9 +193,16 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
           int ys = yy - 1, xs = xx - 1;
           ys = ys < 0 ? ys + n1 : (ys >= n1 ? ys - n1 : ys);
           xs = xs < 0 ? xs + n2 : (xs >= n2 ? xs - n2 : xs);
-          const float* src = xb + (int64_t)ys * n2 + xs;
+          if (gather8) {
+            const int64_t f2 = 2 * n2, fpl = 4 * nplane;
+            const float* src = xb + (int64_t)(2 * ys) * f2 + 2 * xs;
 #pragma unroll
-          for (int c = 0; c < 16; ++c) v[j][c] = __ldg(src + c * nvol);
+            for (int c = 0; c < 8; ++c) v[j][c] = __ldg(src + (c >> 2) * fpl + ((c >> 1) & 1) * f2 + (c & 1));
+          } else {
+            const float* src = xb + (int64_t)ys * n2 + xs;
+#pragma unroll
+            for (int c = 0; c < 16; ++c) v[j][c] = __ldg(src + c * nvol);
+          }
         }
       }
 #pragma unroll
@@ -190,6 +211,7 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
         if (r < PP) {
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
+            if (gather8 && q >= 2) break;
             float h[4], l[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
@@ -225,9 +247,12 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
           const int64_t f2 = 2 * n2, fpl = 4 * nplane;
           float* yp = a.y + band * 8 * nvol + (int64_t)(2 * z) * fpl + (int64_t)(2 * (yy - 1)) * f2 + 2 * (xx - 1);
 #pragma unroll
-          for (int par = 0; par < 8; ++par)
-            yp[(par >> 2) * fpl + ((par >> 1) & 1) * f2 + (par & 1)] +=
-                __uint_as_float(r[par]) + __uint_as_float(r[par + 8]);
+          for (int par = 0; par < 8; ++par) {
+            float* o = yp + (par >> 2) * fpl + ((par >> 1) & 1) * f2 + (par & 1);
+            const float v = __uint_as_float(r[par]) + __uint_as_float(r[par + 8]);
+            if (a.accumulate) *o += v;
+            else *o = v;
+          }
         } else {
           float* yp = a.y + (band * a.cout) * nvol + z * nplane + (int64_t)(yy - 1) * n2 + (xx - 1);
           for (int co = 0; co < a.cout; ++co) {
@@ -275,6 +300,7 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
           const uint32_t off = sbase + (uint32_t)(tb + rowoff[tap / 3] + (tap % 3 - 1));
 #pragma unroll
           for (int c = 0; c < 2; ++c) {
+            if (c == 1 && gather8) break;     // eight input channels: one K = 8 step
             const uint64_t delta = off + 2u * c * (uint32_t)a.npts;
             const uint64_t bw = bw0 + (uint64_t)(tap * 4 * CT_WROWS + c * 2 * CT_WROWS);
             mma_tf32(d, ah0 + delta, bw, idesc, 1u);
@@ -389,6 +415,38 @@ int conv_parity_tc_try(const float* xc, const float* G, float* y, int64_t nb, in
   a.cout = 16;
   a.accumulate = 1;
   return conv_tc_launch(a, nb, n0, n1, n2, st, launched);
+}
+
+// The fine 5^3 stencil of the same level in parity form (mode 2):
+//   y[2J + par] = sum_d F[d] xf[2J + par + d],  d in [-2, 2]^3,
+// xf and y on the fine grid (2 n0, 2 n1, 2 n2).  Writing 2J + par + d =
+// 2 (J + e) + p' (e in {-1,0,1}^3, p' in {0,1}^3, one way for each d) makes
+// it a 3^3 convolution on the coarse grid from the eight parity sub-grids
+// xf[2J + p'] (gathered while staging) to the eight output parities, with
+// weights F[2e + p' - par] (zero outside [-2, 2]^3): one K = 8 step per tap.
+// y is written (not accumulated).
+int conv_fine5_tc_try(const float* xf, const float* F, float* y, int64_t nb, int n0, int n1, int n2,
+                      cudaStream_t st, int* launched) {
+  ConvTcArgs a{};
+  a.x = xf;
+  a.y = y;
+  a.G = F;
+  a.parity = 2;
+  a.cout = 16;
+  a.accumulate = 0;
+  return conv_tc_launch(a, nb, n0, n1, n2, st, launched);
+}
+
+// whether conv_tc_launch takes a coarse grid of this shape
+bool conv_tc_fits(int n0, int n1, int n2) {
+  if (n0 < 2 || n1 < 2 || n2 < 2) return false;
+  const int P2 = n2 + 2, PP = (n1 + 2) * P2, tiles = (PP + 127) / 128;
+  if (tiles > 16) return false;
+  const int m = std::max(P2 + 1, tiles * 128 - PP + P2 + 1);
+  const int npts = PP + 2 * ((m + 7) / 8 * 8);
+  if (npts > 16383) return false;
+  const size_t smem = (size_t)(CT_WFLOATS + 2 * 2 * 4 * npts * 4) * sizeof(float) + 24 + CT_MAXITEMS * sizeof(Item);
+  return smem <= 220 * 1024;
 }
 
 }  // namespace gb

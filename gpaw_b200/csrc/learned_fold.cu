@@ -42,6 +42,9 @@ namespace gb {
 // when the grid does not fit its layout
 int conv_parity_tc_try(const float* xc, const float* G, float* y, int64_t nb, int n0, int n1, int n2,
                        cudaStream_t st, int* launched);
+int conv_fine5_tc_try(const float* xf, const float* F, float* y, int64_t nb, int n0, int n1, int n2,
+                      cudaStream_t st, int* launched);
+bool conv_tc_fits(int n0, int n1, int n2);
 
 namespace {
 
@@ -659,13 +662,21 @@ int gb_learned_fold_fine(const float* xf, const float* F, int rh, const float* x
     return launch_fine(fold_fine_kernel<1, 1>, a, "fold_fine_kernel<1,1>", st);
   }
   if (rh == 2 && cc == 16) {
-    // fine 5^3 part, then the coarse part added as a parity convolution
+    // fine 5^3 part, then the coarse part added as a parity convolution:
+    // both on the tensor cores when the coarse plane fits their layout
+    const int m0 = (int)(n_c[0] / 2), m1 = (int)(n_c[1] / 2), m2 = (int)(n_c[2] / 2);
+    if (conv_tc_fits(m0, m1, m2)) {
+      int launched = 0;
+      int rc = conv_fine5_tc_try(xf, F, y, nb, m0, m1, m2, st, &launched);
+      if (rc) return rc;
+      if (!launched) return fail(GB_E_INVALID, "gb_learned_fold_fine: tensor-core plan refused a fitting grid");
+      rc = conv_parity_tc_try(xc, G, y, nb, m0, m1, m2, st, &launched);
+      if (rc) return rc;
+      if (!launched) return fail(GB_E_INVALID, "gb_learned_fold_fine: tensor-core plan refused a fitting grid");
+      return GB_OK;
+    }
     int rc = launch_fine(fold_fine_kernel<2, 0>, a, "fold_fine_kernel<2,0>", st);
     if (rc) return rc;
-    // on the tensor cores when the coarse plane fits their layout
-    int launched = 0;
-    rc = conv_parity_tc_try(xc, G, y, nb, (int)(n_c[0] / 2), (int)(n_c[1] / 2), (int)(n_c[2] / 2), st, &launched);
-    if (rc || launched) return rc;
     const int m12 = (int)(n_c[1] / 2 * (n_c[2] / 2));
     const unsigned threads = (unsigned)std::min(256, (m12 + 31) / 32 * 32);
     fold_parity16_kernel<<<dim3((unsigned)(n_c[0] / 2), (unsigned)nb), threads, 0, st>>>(a);
