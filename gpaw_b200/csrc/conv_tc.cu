@@ -73,8 +73,8 @@ struct ConvTcArgs {
   const float* x;                 // (nb, 16, n0, n1, n2)
   float* y;                       // (nb, cout, n0, n1, n2)
   const __nv_bfloat16* w;         // [cout][16][27] (plain convolution)
-  const float* G;                 // parity modes: [16][6][6][6] (1) or [5][5][5] (2)
-  int parity;                     // 0: plain; 1, 2: the parity modes (below)
+  const float* G;                 // FP32 weights of modes 1-3: [16][6][6][6], [5][5][5], [5][5][5][16]
+  int parity;                     // 0: plain; 1, 2: the parity modes; 3: the stride-2 mode (below)
   int64_t total;                  // nb n0 output planes
   int cout, n0, n1, n2;
   int P2, PP, tiles, margin, npts, per, accumulate, nissue;
@@ -134,7 +134,16 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
     const int tap = e / (4 * CT_WROWS * 4), r = e % (4 * CT_WROWS * 4);
     const int q = r / (CT_WROWS * 4), n = (r >> 2) % CT_WROWS, i = r & 3;
     const int k = n >> 4, co = n & 15, ci = 4 * q + i;
-    if (a.parity) {
+    if (a.parity == 3) {
+      // output channel co; K step 0 (ci < 8) the TF32 high part of the
+      // weights of input parity ci, K step 1 (ci >= 8) the low part of parity ci - 8
+      const int pp = ci & 7;
+      const int d0 = 2 * (1 - k) + (pp >> 2), d1 = 2 * (tap / 3 - 1) + ((pp >> 1) & 1), d2 = 2 * (tap % 3 - 1) + (pp & 1);
+      const float g = (d0 <= 2 && d1 <= 2 && d2 <= 2) ? __ldg(a.G + (((d0 + 2) * 5 + (d1 + 2)) * 5 + (d2 + 2)) * 16 + co)
+                                                      : 0.f;
+      const float h = rn_tf32(g);
+      sW[e] = ci < 8 ? h : rn_tf32(g - h);
+    } else if (a.parity) {
       // rows 0-7: TF32 high part of the parity-co weights, rows 8-15: the
       // low part; e = (1 - k, tap / 3 - 1, tap % 3 - 1) the coarse offset
       const int par = co & 7;
@@ -177,7 +186,7 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
   // stage the input plane of `it` into slot `sl`, split hi / lo (warps 2-7):
   // a thread takes padded points r, r + 192 (one index division each) and
   // loads all 16 channels of both before it writes any
-  const bool gather8 = a.parity == 2;
+  const bool gather8 = a.parity >= 2;
   auto stage = [&](const Item& it, int sl) {
     // channel c of a plain input: x[band][c][zs]; the eight parity channels
     // p' of a fine input (2 n0, 2 n1, 2 n2): x[band][2 zs + p'0][2 ys + p'1][2 xs + p'2]
@@ -242,7 +251,7 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
       const int lin = t * 128 + 32 * q4 + lane;          // padded point of the plane
       const int yy = lin / P2, xx = lin % P2;
       if (lin < PP && yy >= 1 && yy <= n1 && xx >= 1 && xx <= n2) {
-        if (a.parity) {
+        if (a.parity == 1 || a.parity == 2) {
           // fine grid (2 n0, 2 n1, 2 n2): point 2 J + par gets high + low part
           const int64_t f2 = 2 * n2, fpl = 4 * nplane;
           float* yp = a.y + band * 8 * nvol + (int64_t)(2 * z) * fpl + (int64_t)(2 * (yy - 1)) * f2 + 2 * (xx - 1);
@@ -300,8 +309,9 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
           const uint32_t off = sbase + (uint32_t)(tb + rowoff[tap / 3] + (tap % 3 - 1));
 #pragma unroll
           for (int c = 0; c < 2; ++c) {
-            if (c == 1 && gather8) break;     // eight input channels: one K = 8 step
-            const uint64_t delta = off + 2u * c * (uint32_t)a.npts;
+            if (c == 1 && a.parity == 2) break;   // eight input channels: one K = 8 step
+            // stride mode: both K steps read the eight staged channels
+            const uint64_t delta = off + (a.parity == 3 ? 0u : 2u * c * (uint32_t)a.npts);
             const uint64_t bw = bw0 + (uint64_t)(tap * 4 * CT_WROWS + c * 2 * CT_WROWS);
             mma_tf32(d, ah0 + delta, bw, idesc, 1u);
             mma_tf32(d, al0 + delta, bw, idesc, 1u);
@@ -432,6 +442,25 @@ int conv_fine5_tc_try(const float* xf, const float* F, float* y, int64_t nb, int
   a.y = y;
   a.G = F;
   a.parity = 2;
+  a.cout = 16;
+  a.accumulate = 0;
+  return conv_tc_launch(a, nb, n0, n1, n2, st, launched);
+}
+
+// The stride-2 level-1 -> level-2 stencil of the folded network (mode 3):
+//   y[c][J] = sum_{d in [-2,2]^3} Q[d][c] xf[2J + d],  16 output channels,
+// xf on the fine grid (2 n0, 2 n1, 2 n2), y on the coarse grid.  With
+// d = 2e + p' (e in {-1,0,1}^3, p' in {0,1}^3; d = 3 has no weight) it is
+// a 3^3 convolution from the eight parity sub-grids of xf to 16 channels;
+// the FP32 weights enter as their TF32 high part in K step 0 and their low
+// part in K step 1, both over the same staged channels.  y is written.
+int conv_stride_tc_try(const float* xf, const float* Q, float* y, int64_t nb, int n0, int n1, int n2,
+                       cudaStream_t st, int* launched) {
+  ConvTcArgs a{};
+  a.x = xf;
+  a.y = y;
+  a.G = Q;
+  a.parity = 3;
   a.cout = 16;
   a.accumulate = 0;
   return conv_tc_launch(a, nb, n0, n1, n2, st, launched);

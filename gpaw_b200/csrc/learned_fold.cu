@@ -44,6 +44,8 @@ int conv_parity_tc_try(const float* xc, const float* G, float* y, int64_t nb, in
                        cudaStream_t st, int* launched);
 int conv_fine5_tc_try(const float* xf, const float* F, float* y, int64_t nb, int n0, int n1, int n2,
                       cudaStream_t st, int* launched);
+int conv_stride_tc_try(const float* xf, const float* Q, float* y, int64_t nb, int n0, int n1, int n2,
+                       cudaStream_t st, int* launched);
 bool conv_tc_fits(int n0, int n1, int n2);
 
 namespace {
@@ -692,6 +694,13 @@ int gb_learned_fold_stride(const float* x, const float* Q, float* y, int64_t nb,
   GB_REQUIRE(n_c[0] >= 2 && n_c[1] >= 2 && n_c[2] >= 2 && n_c[0] % 2 == 0 && n_c[1] % 2 == 0 &&
                  n_c[2] % 2 == 0 && n_c[0] < (1 << 20) && n_c[1] < (1 << 20) && n_c[2] < (1 << 20),
              "gb_learned_fold_stride: needs even grid sizes (periodic coarsening)");
+  // on the tensor cores when the coarse plane fits their layout
+  const int m0 = (int)(n_c[0] / 2), m1 = (int)(n_c[1] / 2), m2 = (int)(n_c[2] / 2);
+  if (conv_tc_fits(m0, m1, m2)) {
+    int launched = 0;
+    const int rc = conv_stride_tc_try(x, Q, y, nb, m0, m1, m2, (cudaStream_t)stream, &launched);
+    if (rc || launched) return rc;
+  }
   StrideArgs a{x, y, Q, nb, (int)n_c[0], (int)n_c[1], (int)n_c[2]};
   const int64_t work = nb * (n_c[0] / 2) * (n_c[1] / 2) * ((n_c[2] / 2 + 1) / 2);
   return launch_grid(fold_stride_kernel, a, work, "fold_stride_kernel", (cudaStream_t)stream);
