@@ -345,10 +345,12 @@ static int conv16_launch(const ConvArgs& a, size_t smem, cudaStream_t st) {
 
 // dw[co][ci][k] += sum_b sum_p dy[b][co][p] x[b][ci][p + o_k]   (FP32)
 // grid: (cin * cout channel pairs) x (chunks of the band x point range);
-// each CTA reduces its chunk and adds its 27 sums to dw with atomics
+// each CTA reduces its chunk in a fixed order and writes its 27 sums to
+// part[pair][chunk]; conv3d_bwd_w_reduce_kernel adds them to dw in chunk
+// order, so the gradient does not depend on scheduling
 __global__ void __launch_bounds__(256) conv3d_bwd_w_kernel(const float* __restrict__ x, const float* __restrict__ dy,
-                                                           float* __restrict__ dw, int64_t nb, int cin, int cout, int n0,
-                                                           int n1, int n2, int pbc0, int pbc1, int pbc2) {
+                                                           float* __restrict__ part, int64_t nb, int cin, int cout,
+                                                           int n0, int n1, int n2, int pbc0, int pbc1, int pbc2) {
   const int co = blockIdx.x / cin, ci = blockIdx.x % cin;
   const int64_t n012 = (int64_t)n0 * n1 * n2;
   const int64_t total = nb * n012;
@@ -385,8 +387,20 @@ __global__ void __launch_bounds__(256) conv3d_bwd_w_kernel(const float* __restri
   if (threadIdx.x < 27) {
     float v = 0.f;
     for (int w = 0; w < (int)(blockDim.x / 32); ++w) v += red[w][threadIdx.x];
-    atomicAdd(&dw[((int64_t)co * cin + ci) * 27 + threadIdx.x], v);
+    part[((int64_t)blockIdx.x * gridDim.y + blockIdx.y) * 27 + threadIdx.x] = v;
   }
+}
+
+// dw[pair][k] += sum over chunks c (in order) of part[pair][c][k]
+__global__ void conv3d_bwd_w_reduce_kernel(const float* __restrict__ part, int nchunk, int n,
+                                           float* __restrict__ dw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int pair = i / 27, k = i - pair * 27;
+  const float* p = part + (int64_t)pair * nchunk * 27 + k;
+  float s = 0.f;
+  for (int c = 0; c < nchunk; ++c) s += p[(int64_t)c * 27];
+  dw[i] += s;
 }
 
 template <int CIN, int COUT, int CZT>
@@ -461,11 +475,26 @@ int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw, int64_
   const int64_t total = nb * n_c[0] * n_c[1] * n_c[2];
   const int64_t want = std::max<int64_t>(1, (int64_t)sm_count() * 8 / (cin * cout));
   const int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(want, total / 4096));
-  dim3 grid((unsigned)(cin * cout), (unsigned)std::min<int64_t>(chunks, 65535));
-  conv3d_bwd_w_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(x, dy, dw, nb, cin, cout, (int)n_c[0],
-                                                                    (int)n_c[1], (int)n_c[2], pbc_c[0], pbc_c[1],
-                                                                    pbc_c[2]);
-  return check_launch("conv3d_bwd_w_kernel");
+  const int nchunk = (int)std::min<int64_t>(chunks, 65535);
+  dim3 grid((unsigned)(cin * cout), (unsigned)nchunk);
+  // per-CTA partial sums in stream-ordered memory (freed on the stream
+  // after the reduction), so concurrent calls on different streams do not
+  // share them
+  cudaStream_t st = (cudaStream_t)stream;
+  float* part = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&part), (size_t)cin * cout * nchunk * 27 * sizeof(float), st) !=
+      cudaSuccess)
+    return fail(GB_E_NOMEM, "gb_conv3d_backward_weight: partial-sum allocation failed");
+  conv3d_bwd_w_kernel<<<grid, 256, 0, st>>>(x, dy, part, nb, cin, cout, (int)n_c[0], (int)n_c[1], (int)n_c[2],
+                                            pbc_c[0], pbc_c[1], pbc_c[2]);
+  int rc = check_launch("conv3d_bwd_w_kernel");
+  if (rc == GB_OK) {
+    const int n = cin * cout * 27;
+    conv3d_bwd_w_reduce_kernel<<<(n + 255) / 256, 256, 0, st>>>(part, nchunk, n, dw);
+    rc = check_launch("conv3d_bwd_w_reduce_kernel");
+  }
+  cudaFreeAsync(part, st);
+  return rc;
 }
 
 }  // extern "C"

@@ -116,6 +116,36 @@ __device__ int build_items(const ConvTcArgs& a, int64_t g0, int64_t g1, Item* it
   return n;
 }
 
+// the FP32 weight behind shared-memory element e of the B operands
+// ([9 taps][4 quads][48 rows][4]): row n = 16 k + co, input channel
+// ci = 4 quad + i, z tap 2 - k; the one global load of each element
+__device__ __forceinline__ float weight_raw(const ConvTcArgs& a, int e) {
+  const int tap = e / (4 * CT_WROWS * 4), r = e % (4 * CT_WROWS * 4);
+  const int q = r / (CT_WROWS * 4), n = (r >> 2) % CT_WROWS, i = r & 3;
+  const int k = n >> 4, co = n & 15, ci = 4 * q + i;
+  const int e0 = 1 - k, e1 = tap / 3 - 1, e2 = tap % 3 - 1;   // coarse offset of the tap
+  if (a.parity == 0)
+    return co < a.cout ? __bfloat162float(a.w[(co * 16 + ci) * 27 + 9 * (2 - k) + tap]) : 0.f;
+  if (a.parity == 3) {
+    // output channel co, input parity ci & 7: fine offset d = 2e + p'
+    const int pp = ci & 7;
+    const int d0 = 2 * e0 + (pp >> 2), d1 = 2 * e1 + ((pp >> 1) & 1), d2 = 2 * e2 + (pp & 1);
+    return (d0 <= 2 && d1 <= 2 && d2 <= 2) ? __ldg(a.G + (((d0 + 2) * 5 + (d1 + 2)) * 5 + (d2 + 2)) * 16 + co) : 0.f;
+  }
+  const int par = co & 7;
+  if (a.parity == 1) {
+    const int tx = (par >> 2) - 2 * e0 + 2, ty = ((par >> 1) & 1) - 2 * e1 + 2, tz = (par & 1) - 2 * e2 + 2;
+    return (tx < 5 && ty < 5 && tz < 5) ? __ldg(a.G + ci * 216 + (tx * 6 + ty) * 6 + tz) : 0.f;
+  }
+  if (ci >= 8) return 0.f;
+  // fine offset d = 2e + p' - par of input parity p' = ci
+  const int d0 = 2 * e0 + (ci >> 2) - (par >> 2), d1 = 2 * e1 + ((ci >> 1) & 1) - ((par >> 1) & 1);
+  const int d2 = 2 * e2 + (ci & 1) - (par & 1);
+  return (d0 >= -2 && d0 <= 2 && d1 >= -2 && d1 <= 2 && d2 >= -2 && d2 <= 2)
+             ? __ldg(a.G + ((d0 + 2) * 5 + (d1 + 2)) * 5 + (d2 + 2))
+             : 0.f;
+}
+
 __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcArgs a) {
   extern __shared__ __align__(128) unsigned char ctc_smem[];
   float* sW = reinterpret_cast<float*>(ctc_smem);              // [9 taps][4 quads][48 rows][4]
@@ -130,39 +160,26 @@ __global__ void __launch_bounds__(CT_THREADS, 2) conv16_tc_kernel(const ConvTcAr
   const int n0 = a.n0, n1 = a.n1, n2 = a.n2, P2 = a.P2, PP = a.PP;
   const int64_t g0 = (int64_t)blockIdx.x * a.per, g1 = min(a.total, g0 + a.per);
 
-  for (int e = tid; e < CT_WFLOATS; e += CT_THREADS) {
-    const int tap = e / (4 * CT_WROWS * 4), r = e % (4 * CT_WROWS * 4);
-    const int q = r / (CT_WROWS * 4), n = (r >> 2) % CT_WROWS, i = r & 3;
-    const int k = n >> 4, co = n & 15, ci = 4 * q + i;
-    if (a.parity == 3) {
-      // output channel co; K step 0 (ci < 8) the TF32 high part of the
-      // weights of input parity ci, K step 1 (ci >= 8) the low part of parity ci - 8
-      const int pp = ci & 7;
-      const int d0 = 2 * (1 - k) + (pp >> 2), d1 = 2 * (tap / 3 - 1) + ((pp >> 1) & 1), d2 = 2 * (tap % 3 - 1) + (pp & 1);
-      const float g = (d0 <= 2 && d1 <= 2 && d2 <= 2) ? __ldg(a.G + (((d0 + 2) * 5 + (d1 + 2)) * 5 + (d2 + 2)) * 16 + co)
-                                                      : 0.f;
-      const float h = rn_tf32(g);
-      sW[e] = ci < 8 ? h : rn_tf32(g - h);
-    } else if (a.parity) {
-      // rows 0-7: TF32 high part of the parity-co weights, rows 8-15: the
-      // low part; e = (1 - k, tap / 3 - 1, tap % 3 - 1) the coarse offset
-      const int par = co & 7;
-      const int e0 = 1 - k, e1 = tap / 3 - 1, e2 = tap % 3 - 1;
-      float g = 0.f;
-      if (a.parity == 1) {
-        const int tx = (par >> 2) - 2 * e0 + 2, ty = ((par >> 1) & 1) - 2 * e1 + 2, tz = (par & 1) - 2 * e2 + 2;
-        if (tx < 5 && ty < 5 && tz < 5) g = __ldg(a.G + ci * 216 + (tx * 6 + ty) * 6 + tz);
-      } else if (ci < 8) {
-        // fine offset d = 2 e + p' - par of input parity p' = ci
-        const int d0 = 2 * e0 + (ci >> 2) - (par >> 2), d1 = 2 * e1 + ((ci >> 1) & 1) - ((par >> 1) & 1);
-        const int d2 = 2 * e2 + (ci & 1) - (par & 1);
-        if (d0 >= -2 && d0 <= 2 && d1 >= -2 && d1 <= 2 && d2 >= -2 && d2 <= 2)
-          g = __ldg(a.G + ((d0 + 2) * 5 + (d1 + 2)) * 5 + (d2 + 2));
+  {
+    // weights: all of a thread's 27 loads are issued before any is used
+    // (one L2 round trip for the prologue instead of 27 in a row)
+    constexpr int WPER = CT_WFLOATS / CT_THREADS;
+    float wv[WPER];
+#pragma unroll
+    for (int u = 0; u < WPER; ++u) wv[u] = weight_raw(a, tid + u * CT_THREADS);
+#pragma unroll
+    for (int u = 0; u < WPER; ++u) {
+      const int e = tid + u * CT_THREADS;
+      const float g = wv[u];
+      if (a.parity) {
+        // hi part in rows 0-7 (parity modes) or K step 0 (stride mode), lo part in the rest
+        const int n = (e >> 2) % CT_WROWS, ci = 4 * ((e % (4 * CT_WROWS * 4)) / (CT_WROWS * 4)) + (e & 3);
+        const bool hi = a.parity == 3 ? ci < 8 : (n & 15) < 8;
+        const float h = rn_tf32(g);
+        sW[e] = hi ? h : rn_tf32(g - h);
+      } else {
+        sW[e] = g;
       }
-      const float h = rn_tf32(g);
-      sW[e] = co < 8 ? h : rn_tf32(g - h);
-    } else {
-      sW[e] = co < a.cout ? __bfloat162float(a.w[(co * 16 + ci) * 27 + 9 * (2 - k) + tap]) : 0.f;
     }
   }
   // margins of both slots and every quad: zero (only dropped halo outputs read them)

@@ -1,7 +1,7 @@
 """GPU: the learned preconditioner's forward and backward kernels against
 the FP64 oracle (oracle/learned.py) with the same BF16-rounded weights
 (tolerance 1e-4 norm-wise relative: FP32 activations and accumulation),
-and training on (residual, multigrid correction) pairs lowers the loss."""
+weight gradients that repeat bit for bit, and training on (residual, multigrid correction) pairs lowers the loss."""
 import numpy as np
 import pytest
 import torch
@@ -39,6 +39,10 @@ def test_forward_backward_vs_oracle(N, pbc):
     assert abs(loss - oloss) < 1e-4 * abs(oloss)
     for k in grads:
         assert rel(grads[k].double().cpu().numpy(), ograds[k]) < 1e-3, k
+    # the weight gradients are reduced in a fixed order: bit-identical repeats
+    again = net.backward(g)
+    for k in grads:
+        assert torch.equal(grads[k], again[k]), k
 
 
 def test_training_reduces_loss():
