@@ -540,6 +540,16 @@ static int restrict_cfg(const gb_transformer* t, const void* in, void* out, int6
 // points (axis 2, then axis 1: the general kernel's arithmetic, in its
 // order) and the axis-0 step takes the last three fine planes from a
 // register queue.  Rows must be 16-byte aligned.
+// four consecutive values from a 16-byte aligned shared-memory address
+__device__ __forceinline__ void load4(const float* f, float (&v)[4]) {
+  const float4 q = *reinterpret_cast<const float4*>(f);
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void load4(const double* f, double (&v)[4]) {
+  const double2 q0 = reinterpret_cast<const double2*>(f)[0], q1 = reinterpret_cast<const double2*>(f)[1];
+  v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+}
+
 template <typename T, int TYC>
 __global__ void __launch_bounds__(256) restrict2_march_kernel(const TrArgs a, int nch) {
   extern __shared__ __align__(16) unsigned char r2m_smem[];
@@ -559,10 +569,43 @@ __global__ void __launch_bounds__(256) restrict2_march_kernel(const TrArgs a, in
   const T w0 = (T)a.w[0], half = (T)0.5, alpha = (T)a.alpha;
   const int r0 = 2 * J0 + a.off[1] - 1;                 // first staged fine row
   auto wrap = [](int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); };
+  // the copies of a staged plane: element e = (row r, piece c) is a 16-byte
+  // chunk (c < chunks), column -1 or column nf2; a thread's first MAXU
+  // elements have their offsets worked out once (no index divisions per plane)
+  const int chunks = nf2 / VEC, ne = FR * (chunks + 2);
+  constexpr int MAXU = 4;
+  int s_off[MAXU], d_off[MAXU];
+  unsigned wide = 0u;
+#pragma unroll
+  for (int u = 0; u < MAXU; ++u) {
+    const int e = tid + u * nt;
+    s_off[u] = 0;
+    d_off[u] = -1;
+    if (e < ne) {
+      const int r = e / (chunks + 2), c = e % (chunks + 2);
+      const int row = wrap(r0 + r, nf1) * nf2;
+      if (c < chunks) {
+        s_off[u] = row + c * VEC;
+        d_off[u] = r * FP + VEC + c * VEC;
+        wide |= 1u << u;
+      } else if (c == chunks) {
+        s_off[u] = row + nf2 - 1;                 // column -1
+        d_off[u] = r * FP + VEC - 1;
+      } else {
+        s_off[u] = row;                           // column nf2
+        d_off[u] = r * FP + VEC + nf2;
+      }
+    }
+  }
   auto stage = [&](int p, T* d) {
     const T* pl = src + (int64_t)wrap(p, nf0) * nf1 * nf2;
-    const int chunks = nf2 / VEC;
-    for (int e = tid; e < FR * (chunks + 2); e += nt) {
+#pragma unroll
+    for (int u = 0; u < MAXU; ++u) {
+      if (d_off[u] < 0) continue;
+      if (wide & (1u << u)) cp_async16(d + d_off[u], pl + s_off[u]);
+      else cp_async_elem(d + d_off[u], pl + s_off[u]);
+    }
+    for (int e = tid + MAXU * nt; e < ne; e += nt) {
       const int r = e / (chunks + 2), c = e % (chunks + 2);
       const T* row = pl + (int64_t)wrap(r0 + r, nf1) * nf2;
       T* dr = d + r * FP;
@@ -571,6 +614,9 @@ __global__ void __launch_bounds__(256) restrict2_march_kernel(const TrArgs a, in
       else cp_async_elem(dr + VEC + nf2, row);                          // column nf2
     }
   };
+  // the five fine columns 2K - 1 .. 2K + 3 a thread reads per row: one
+  // 16-byte load and one scalar when the window start is 16-byte aligned
+  const bool vec4 = (a.off[2] % VEC) == 0;
   const int p_beg = 2 * I_beg + a.off[0] - 1, p_end = 2 * (I_end - 1) + a.off[0] + 1;
   stage(p_beg, slot);
   cp_async_commit();
@@ -588,9 +634,16 @@ __global__ void __launch_bounds__(256) restrict2_march_kernel(const TrArgs a, in
 #pragma unroll
       for (int dy = 0; dy < 3; ++dy) {
         const T* f = P + dy * FP;
+        T v[4];
+        if (vec4) {
+          load4(f, v);
+        } else {
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
-          g[dy][h] = half * fmadd(f[2 * h], w0, add(f[2 * h + 1], f[2 * h - 1]));
+          for (int i = 0; i < 4; ++i) v[i] = f[i];
+        }
+        const T fm = f[-1];
+        g[dy][0] = half * fmadd(v[0], w0, add(v[1], fm));
+        g[dy][1] = half * fmadd(v[2], w0, add(v[3], v[1]));
       }
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
