@@ -728,15 +728,26 @@ __global__ void __launch_bounds__(256) interp2_march_kernel(const TrArgs a, int 
   const T* ysrc = a.y ? reinterpret_cast<const T*>(a.y) + b * 2 * (int64_t)nc0 * fplane : nullptr;
   const T w0 = (T)a.w[0], alpha = (T)a.alpha, gamma = (T)a.gamma;
   auto wrap = [](int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); };
+  // rows of a whole number of 16-byte chunks are copied in chunks, others
+  // (a 14-point FP32 row, say) element by element
+  const bool rows16 = (nc2 * (int)sizeof(T)) % 16 == 0;
   auto stage = [&](int g, T* d) {
     const T* pl = src + (int64_t)wrap(g, nc0) * nc1 * nc2;
-    const int chunks = nc2 / VEC;
-    for (int e = tid; e < CRR * (chunks + 1); e += nt) {
-      const int r = e / (chunks + 1), c = e % (chunks + 1);
-      const T* row = pl + (int64_t)wrap((F0 >> 1) + r, nc1) * nc2;
-      T* dr = d + r * CP;
-      if (c < chunks) cp_async16(dr + VEC + c * VEC, row + c * VEC);
-      else cp_async_elem(dr + VEC + nc2, row);                 // column nc2
+    if (rows16) {
+      const int chunks = nc2 / VEC;
+      for (int e = tid; e < CRR * (chunks + 1); e += nt) {
+        const int r = e / (chunks + 1), c = e % (chunks + 1);
+        const T* row = pl + (int64_t)wrap((F0 >> 1) + r, nc1) * nc2;
+        T* dr = d + r * CP;
+        if (c < chunks) cp_async16(dr + VEC + c * VEC, row + c * VEC);
+        else cp_async_elem(dr + VEC + nc2, row);                 // column nc2
+      }
+    } else {
+      for (int e = tid; e < CRR * (nc2 + 1); e += nt) {
+        const int r = e / (nc2 + 1), c = e % (nc2 + 1);
+        const T* row = pl + (int64_t)wrap((F0 >> 1) + r, nc1) * nc2;
+        cp_async_elem(d + r * CP + VEC + c, row + (c < nc2 ? c : 0));   // column nc2 = column 0
+      }
     }
   };
   stage(C_beg, slot);
@@ -806,8 +817,8 @@ static bool interp2_march_ok(const gb_transformer* t, int64_t nin, const double*
   const int64_t ngx = nf2 / 4;
   const int64_t tyf = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
   (void)y;
-  return (nc2 * (int64_t)sizeof(T)) % 16 == 0 && nf2 % 4 == 0 && ngx * 2 <= 256 && t->nin_c[0] >= 1 &&
-         t->nin_c[1] >= tyf / 2 + 1 && nc2 >= 16 / (int)sizeof(T);
+  return nf2 % 4 == 0 && ngx * 2 <= 256 && t->nin_c[0] >= 1 && t->nin_c[1] >= tyf / 2 + 1 &&
+         nc2 >= 16 / (int)sizeof(T);
 }
 
 template <typename T>

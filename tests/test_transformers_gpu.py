@@ -44,6 +44,7 @@ def test_golden_transformers(golden_kernels):
                                    ((32, 32, 32), (1, 1, 1)),
                                    ((24, 40, 16), (1, 0, 1)),
                                    ((56, 56, 56), (1, 1, 1)),
+                                   ((28, 28, 28), (1, 1, 1)),
                                    ((76, 20, 12), (0, 0, 0))])
 @pytest.mark.parametrize('nn', [1, 2, 3, 4])
 @pytest.mark.parametrize('dtype', [torch.float64, torch.float32,
