@@ -842,11 +842,195 @@ static int interp2_march_launch(const gb_transformer* t, const void* in, void* o
 
 // coarse rows of at most 16 points (the coarse levels of small grids) use a
 // 16 x 16 tile, wider ones 8 x 32: no more than half a warp idles on a row
+// k = 6 restriction of real data on a grid periodic on every axis (the
+// density / potential transfers between the coarse and the fine grid),
+// marching along axis 0 like restrict2_march_kernel: a CTA owns TYC coarse
+// rows of one band over a chunk of coarse planes and stages every fine
+// plane it needs once (rows 2 J0 + off - 5 .. 2 (J0 + TYC - 1) + off + 5,
+// five wrap-around columns on each side) with cp.async into a two-slot
+// ring.  A thread restricts the plane in-plane for two neighbouring coarse
+// points -- axis 2 on each of its seven fine rows, then axis 1 -- and the
+// axis-0 step takes the last eleven fine planes from a register queue; the
+// arithmetic of the general kernel (x = f0, x += w_m (f_{2m+1} + f_{-2m-1}),
+// m = 0, 1, 2, then x / 2, axis by axis), in its order.  Rows must be
+// 16-byte aligned.
+template <typename T, int TYC>
+__global__ void __launch_bounds__(256) restrict6_march_kernel(const TrArgs a, int nch) {
+  extern __shared__ __align__(16) unsigned char r6m_smem[];
+  T* slot = reinterpret_cast<T*>(r6m_smem);
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int CO = ((5 + VEC - 1) / VEC) * VEC;        // fine column c at CO + c
+  const int nf0 = a.ni[0], nf1 = a.ni[1], nf2 = a.ni[2];
+  const int nc0 = a.no[0], nc1 = a.no[1], nc2 = a.no[2];
+  const int FR = 2 * TYC + 9, FP = nf2 + 2 * CO + 2 * VEC;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int ngx = (nc2 + 1) >> 1;
+  const int gx = tid % ngx, ty = tid / ngx;
+  const int J0 = blockIdx.y * TYC, J = J0 + ty, K0 = 2 * gx;
+  const int64_t b = blockIdx.z;
+  const int I_beg = (int)((int64_t)blockIdx.x * nc0 / nch), I_end = (int)((int64_t)(blockIdx.x + 1) * nc0 / nch);
+  const T* src = reinterpret_cast<const T*>(a.in) + b * (int64_t)nf0 * nf1 * nf2;
+  T* dst = reinterpret_cast<T*>(a.out) + b * (int64_t)nc0 * nc1 * nc2;
+  const T w0 = (T)a.w[0], w1 = (T)a.w[1], w2 = (T)a.w[2], half = (T)0.5, alpha = (T)a.alpha;
+  const int r0 = 2 * J0 + a.off[1] - 5;                 // first staged fine row
+  auto wrap = [](int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); };
+  // element e = (row r, piece c): 16-byte chunks c < chunks, then the five
+  // columns -5 .. -1 and the five columns nf2 .. nf2 + 4
+  const int chunks = nf2 / VEC, per = chunks + 10, ne = FR * per;
+  constexpr int MAXU = 8;
+  int s_off[MAXU], d_off[MAXU];
+  unsigned wide = 0u;
+#pragma unroll
+  for (int u = 0; u < MAXU; ++u) {
+    const int e = tid + u * nt;
+    s_off[u] = 0;
+    d_off[u] = -1;
+    if (e < ne) {
+      const int r = e / per, c = e % per;
+      const int row = wrap(r0 + r, nf1) * nf2;
+      if (c < chunks) {
+        s_off[u] = row + c * VEC;
+        d_off[u] = r * FP + CO + c * VEC;
+        wide |= 1u << u;
+      } else if (c < chunks + 5) {
+        const int h = c - chunks;                   // column h - 5
+        s_off[u] = row + nf2 - 5 + h;
+        d_off[u] = r * FP + CO - 5 + h;
+      } else {
+        const int h = c - chunks - 5;               // column nf2 + h
+        s_off[u] = row + h;
+        d_off[u] = r * FP + CO + nf2 + h;
+      }
+    }
+  }
+  auto stage = [&](int p, T* d) {
+    const T* pl = src + (int64_t)wrap(p, nf0) * nf1 * nf2;
+#pragma unroll
+    for (int u = 0; u < MAXU; ++u) {
+      if (d_off[u] < 0) continue;
+      if (wide & (1u << u)) cp_async16(d + d_off[u], pl + s_off[u]);
+      else cp_async_elem(d + d_off[u], pl + s_off[u]);
+    }
+    for (int e = tid + MAXU * nt; e < ne; e += nt) {
+      const int r = e / per, c = e % per;
+      const T* row = pl + (int64_t)wrap(r0 + r, nf1) * nf2;
+      T* dr = d + r * FP + CO;
+      if (c < chunks) cp_async16(dr + c * VEC, row + c * VEC);
+      else if (c < chunks + 5) cp_async_elem(dr - 5 + (c - chunks), row + nf2 - 5 + (c - chunks));
+      else cp_async_elem(dr + nf2 + (c - chunks - 5), row + (c - chunks - 5));
+    }
+  };
+  // one axis: x = f0; x += w_m (f_{2m+1} + f_{-(2m+1)}); x / 2
+  auto axis = [&](T c0, T p1, T m1, T p3, T m3, T p5, T m5) {
+    T x = c0;
+    x = fmadd(x, w0, add(p1, m1));
+    x = fmadd(x, w1, add(p3, m3));
+    x = fmadd(x, w2, add(p5, m5));
+    return half * x;
+  };
+  const int p_beg = 2 * I_beg + a.off[0] - 5, p_end = 2 * (I_end - 1) + a.off[0] + 5;
+  stage(p_beg, slot);
+  cp_async_commit();
+  T q[2][11];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int m = 0; m < 11; ++m) q[h][m] = (T)0;
+  const bool act = ty < TYC && J < nc1;
+  for (int p = p_beg; p <= p_end; ++p) {
+    const int s = (p - p_beg) & 1;
+    if (p + 1 <= p_end) stage(p + 1, slot + (s ^ 1) * FR * FP);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    if (act) {
+      // centre fine row 2J + off of this thread: staged row 2 ty + 5
+      const T* P = slot + s * FR * FP + (2 * ty + 5) * FP + CO + 2 * K0 + a.off[2];
+      T g[2][11];                                      // [h][fine row offset + 5]
+#pragma unroll
+      for (int dy = -5; dy <= 5; ++dy) {
+        if (dy != 0 && (dy & 1) == 0) continue;        // even offsets carry no weight
+        const T* f = P + dy * FP;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const T* c = f + 2 * h;
+          g[h][dy + 5] = axis(c[0], c[1], c[-1], c[3], c[-3], c[5], c[-5]);
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+#pragma unroll
+        for (int m = 0; m < 10; ++m) q[h][m] = q[h][m + 1];
+        q[h][10] = axis(g[h][5], g[h][6], g[h][4], g[h][8], g[h][2], g[h][10], g[h][0]);
+      }
+      const int tI = p - a.off[0] - 5;                  // fine plane 2I + off + 5 just arrived
+      if (tI >= 2 * I_beg && (tI & 1) == 0) {
+        const int I = tI >> 1;
+        T* o = dst + ((int64_t)I * nc1 + J) * nc2 + K0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (K0 + h < nc2) o[h] = alpha * axis(q[h][5], q[h][6], q[h][4], q[h][8], q[h][2], q[h][10], q[h][0]);
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+}
+
+template <typename T>
+static bool restrict6_march_ok(const gb_transformer* t, int64_t nin, const double* ph) {
+  if (!t->pbc[0] || !t->pbc[1] || !t->pbc[2] || nin > 65535 || nin < 1) return false;
+  if (ph)
+    for (int i = 0; i < 12; ++i)
+      if (ph[i] != ((i % 2) ? 0.0 : 1.0)) return false;
+  const int64_t nf2 = t->nin_c[2];
+  const int64_t ngx = (t->nout_c[2] + 1) / 2;
+  const int64_t tyc = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
+  // single-wrap periodic indices: at least 6 fine planes and columns, and
+  // rows enough that the last tile's staged rows (up to nf1 + 2 TYC + 2)
+  // stay below 2 nf1
+  return (nf2 * (int64_t)sizeof(T)) % 16 == 0 && ngx * 2 <= 256 && t->nin_c[0] >= 6 &&
+         t->nin_c[1] >= 2 * tyc + 3 && nf2 >= 6 && t->nout_c[1] >= 1 && t->nout_c[0] >= 1;
+}
+
+template <typename T>
+static int restrict6_march_launch(const gb_transformer* t, const void* in, void* out, int64_t nin,
+                                  cudaStream_t st, double alpha) {
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int CO = ((5 + VEC - 1) / VEC) * VEC;
+  TrArgs a;
+  fill_common(t, a, nullptr, 1, nin);
+  a.in = in; a.out = out; a.nbatch = nin; a.alpha = alpha;
+  const int ngx = (a.no[2] + 1) / 2;
+  const int TYC = ngx * 8 <= 256 ? 8 : (ngx * 4 <= 256 ? 4 : 2);
+  // plane chunks: enough CTAs for every SM (a single grid is cut into
+  // short chunks, each re-staging its ten halo planes from L2)
+  const int64_t tiles = (int64_t)((a.no[1] + TYC - 1) / TYC) * nin;
+  const int nch = (int)std::max<int64_t>(1, std::min<int64_t>(a.no[0], (sm_count() + tiles - 1) / tiles));
+  const size_t smem = (size_t)2 * (2 * TYC + 9) * (a.ni[2] + 2 * CO + 2 * VEC) * sizeof(T);
+  static size_t attr = 0;
+  if (smem > 48 * 1024 && smem > attr) {
+    cudaFuncSetAttribute(restrict6_march_kernel<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(restrict6_march_kernel<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(restrict6_march_kernel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = smem;
+  }
+  const dim3 grid((unsigned)nch, (unsigned)((a.no[1] + TYC - 1) / TYC), (unsigned)nin);
+  const unsigned threads = (unsigned)(ngx * TYC);
+  if (TYC == 8) restrict6_march_kernel<T, 8><<<grid, threads, smem, st>>>(a, nch);
+  else if (TYC == 4) restrict6_march_kernel<T, 4><<<grid, threads, smem, st>>>(a, nch);
+  else restrict6_march_kernel<T, 2><<<grid, threads, smem, st>>>(a, nch);
+  return check_launch("restrict6_march_kernel");
+}
+
 template <typename T, int K>
 static int restrict_k(const gb_transformer* t, const void* in, void* out, int64_t nin,
                       const double* ph, cudaStream_t st, double alpha, int nk) {
   if constexpr (K == 2 && !Elem<T>::cplx) {
     if (restrict2_march_ok<T>(t, nin, ph)) return restrict2_march_launch<T>(t, in, out, nin, st, alpha);
+  }
+  if constexpr (K == 6 && !Elem<T>::cplx) {
+    if (restrict6_march_ok<T>(t, nin, ph)) return restrict6_march_launch<T>(t, in, out, nin, st, alpha);
   }
   if (t->nout_c[2] <= 16) return restrict_cfg<T, K, 16, 16>(t, in, out, nin, ph, st, alpha, nk);
   return restrict_cfg<T, K, 8, 32>(t, in, out, nin, ph, st, alpha, nk);
