@@ -22,6 +22,7 @@
 // sums and adds them to dw with FP32 atomics (dw accumulates, as before).
 #include <cuda_bf16.h>
 #include <algorithm>
+#include <mutex>
 #include "internal.cuh"
 
 namespace gb {
@@ -431,6 +432,28 @@ static int fwd_launch(const ConvArgs& a, cudaStream_t st) {
 
 using namespace gb;
 
+// the memory pool of the weight-gradient partial sums on the current
+// device (created once, release threshold unlimited); null on failure
+static cudaMemPool_t part_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
 extern "C" {
 
 int gb_conv3d_forward(const float* x, const void* w_bf16, float* y, int64_t nb, int cin, int cout,
@@ -479,11 +502,13 @@ int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw, int64_
   dim3 grid((unsigned)(cin * cout), (unsigned)nchunk);
   // per-CTA partial sums in stream-ordered memory (freed on the stream
   // after the reduction), so concurrent calls on different streams do not
-  // share them
+  // share them; from a pool of this library that keeps freed memory, so
+  // the thousands of calls of a training run do not map and unmap it
   cudaStream_t st = (cudaStream_t)stream;
+  cudaMemPool_t pool = part_pool();
   float* part = nullptr;
-  if (cudaMallocAsync(reinterpret_cast<void**>(&part), (size_t)cin * cout * nchunk * 27 * sizeof(float), st) !=
-      cudaSuccess)
+  if (!pool || cudaMallocFromPoolAsync(reinterpret_cast<void**>(&part),
+                                       (size_t)cin * cout * nchunk * 27 * sizeof(float), pool, st) != cudaSuccess)
     return fail(GB_E_NOMEM, "gb_conv3d_backward_weight: partial-sum allocation failed");
   conv3d_bwd_w_kernel<<<grid, 256, 0, st>>>(x, dy, part, nb, cin, cout, (int)n_c[0], (int)n_c[1], (int)n_c[2],
                                             pbc_c[0], pbc_c[1], pbc_c[2]);
