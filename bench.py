@@ -501,6 +501,58 @@ def lfc_benchmark(args):
                       'add_us': round(t_add, 1), 'integrate_us': round(t_int, 1)}))
 
 
+def iteration_profile(args):
+    """Kernel-by-kernel device time of one Si64 SCF iteration in the two FP32
+    forms (learned and multigrid preconditioner), graph-replayed: the Si64
+    FP32 calculation of scf_benchmark, the network initialised from the
+    V-cycle (its cost does not depend on the weights), iterations 13-17 of
+    a run timed with the torch profiler's CUDA kernel records (graph kernels
+    included).  Prints one JSON object: per form the device time per
+    iteration, the median wall time per iteration and the 40 costliest
+    kernels (microseconds and launches per iteration)."""
+    import numpy as np
+    import torch
+    from torch.profiler import profile, ProfilerActivity
+    from gpaw_b200.scf import Calculation, si_diamond
+    from gpaw_b200.learned import ConvNet, LearnedPreconditioner
+    k0, k = 12, 5
+    out = {'workload': 'Si64 (56^3, 160 FP32 bands, LDA, Gamma), one graph-replayed SCF '
+                       f'iteration, mean of iterations {k0 + 1}-{k0 + k}'}
+    for learned in (True, False):
+        sym, pos, cell = si_diamond(2, 5.43, rattle=0.05, seed=0)
+        c = Calculation(sym, pos, cell, True, h=0.2, nbands=160, xc='LDA', precision='fp32')
+        if learned:
+            net = ConvNet(c.gd, seed=0).init_from_multigrid(c.preconditioner)
+            c.use_preconditioner(LearnedPreconditioner(net, c.preconditioner))
+        prof = profile(activities=[ProfilerActivity.CUDA])
+
+        def window(calc, it, log):
+            if it == k0:
+                torch.cuda.synchronize()
+                prof.start()
+            if it == k0 + k:
+                torch.cuda.synchronize()
+                prof.stop()
+        log = c.run(maxiter=k0 + k, energy_tol=0.0, callback=window, graph=True)
+        rows = []
+        for e in prof.key_averages():
+            t = getattr(e, 'self_device_time_total', None)
+            if t is None:
+                t = e.self_cuda_time_total
+            if t > 0:
+                rows.append((t / k, e.count / k, e.key))
+        rows.sort(reverse=True)
+        wall = np.diff(np.r_[0.0, log.times])[k0:]
+        out['learned' if learned else 'multigrid'] = {
+            'device_us_per_iteration': round(sum(r[0] for r in rows), 1),
+            'wall_ms_median': round(float(np.median(wall)) * 1e3, 2),
+            'fallback_at': log.fallback_at,
+            'kernels': [(round(t, 1), round(n, 2), name) for t, n, name in rows[:40]]}
+        del c, prof
+        gc.collect()
+    print(json.dumps(out))
+
+
 def network_benchmark(args):
     """The learned preconditioner's forward pass on its production shape:
     160 FP32 residuals of the 56^3 periodic Si64 grid (h = 0.194 A), the
@@ -667,6 +719,10 @@ def main():
                     help='time the learned preconditioner network alone: one '
                          'forward pass over 160 FP32 residuals of the 56^3 Si64 '
                          'grid per step (the command line used for ncu captures)')
+    ap.add_argument('--iteration-profile', action='store_true',
+                    help='kernel-by-kernel device time of one graph-replayed Si64 '
+                         'FP32 SCF iteration, learned and multigrid forms (torch '
+                         'profiler; the command behind the iteration summary)')
     ap.add_argument('--lfc-only', action='store_true',
                     help='time the projector LFC add and integrate alone on the '
                          'Si64 shape (64 atoms x 8 functions, 160 FP32 bands of '
@@ -695,6 +751,9 @@ def main():
         return
     if args.network_only:
         network_benchmark(args)
+        return
+    if args.iteration_profile:
+        iteration_profile(args)
         return
     if args.lfc_only:
         lfc_benchmark(args)
