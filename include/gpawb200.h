@@ -318,6 +318,9 @@ int gb_conv3d_forward(const float* x, const void* w_bf16, float* y,
 int gb_conv3d_forward_pair(const float* x0, const float* x1, const void* w_bf16,
                            float* y, int64_t nb, const int64_t n_c[3],
                            const int pbc_c[3], void* stream);
+/* dw += dL/dw summed in a fixed order (bit-identical on repeats); the
+ * per-block partial sums live in stream-ordered memory from a pool of this
+ * library that keeps what it frees (GB_E_NOMEM if that allocation fails). */
 int gb_conv3d_backward_weight(const float* x, const float* dy, float* dw,
                               int64_t nb, int cin, int cout,
                               const int64_t n_c[3], const int pbc_c[3],
